@@ -1,0 +1,46 @@
+"""Extract the reference's golden vectors for the Omniscape path into small fixtures.
+
+Run in a checkout that has the reference sources (``--ref`` points at the
+landschaft source tree).  Reads the reference's own test data:
+
+* ``tests/data/reference/circuit/omniscape.npz``: 8 Omniscape.jl 0.7 runs
+  (inputs, options and the CHOLMOD outputs; the cg+amg outputs are left out);
+* ``tests/data/reference/circuit/advanced.npz`` + ``advanced_inputs.npz``: 6
+  Circuitscape advanced-mode solves (CHOLMOD node currents).
+
+Writes ``omniscape_golden.npz`` and ``advanced_golden.npz`` next to this file.
+The GPU machines do not have the reference tree, so the tests read only these
+fixtures.
+"""
+
+from __future__ import annotations
+
+import argparse
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    args = ap.parse_args()
+    data = Path(args.ref) / "tests" / "data" / "reference" / "circuit"
+    z = np.load(data / "omniscape.npz")
+    out = {}
+    for k in z.files:
+        if "/cgamg/" in k:
+            continue
+        out[k] = z[k]
+    np.savez_compressed(HERE / "omniscape_golden.npz", **out)
+    inp = np.load(data / "advanced_inputs.npz")
+    ref = np.load(data / "advanced.npz")
+    out = {k: inp[k] for k in inp.files}
+    out.update({k: ref[k] for k in ref.files if k.endswith("current_cholmod")})
+    np.savez_compressed(HERE / "advanced_golden.npz", **out)
+
+
+if __name__ == "__main__":
+    main()
