@@ -1,0 +1,160 @@
+/*
+ * lsb_omniscape.h -- C ABI of landschaft_b200's Omniscape moving-window
+ * circuit solver on one B200 (sm_100a).
+ *
+ * Plain C types only: pointers, sizes, a parameter struct.  No exceptions
+ * cross this boundary; every entry point returns LSB_OK (0) or an error code,
+ * with a message in `err` when err != NULL.
+ *
+ * Reference interfaces replaced (paths within the landschaft source tree):
+ *   lsb_omniscape               circuit_omniscape  src/cpp/circuit/python.cpp:90-137
+ *                               -> circuit::omniscape  src/cpp/circuit/omniscape.hpp:56-60
+ *   lsb_omniscape_correction    circuit_omniscape_correction  src/cpp/circuit/python.cpp:139-153
+ *                               -> circuit::omniscape_correction  src/cpp/circuit/omniscape.hpp:62-64
+ *   lsb_omniscape_grad          (no reference counterpart: adjoint of the cumulative current)
+ *   lsb_params_default          OmniscapeParams defaults  src/cpp/circuit/omniscape.hpp:35-47
+ *
+ * Memory: resistance, source, condition rasters and every output are DEVICE
+ * pointers (row-major ny x nx float64).  The caller owns them and a device
+ * workspace of lsb_omniscape_workspace_size() bytes; the library allocates
+ * nothing on the device during a call.  Work is enqueued on `stream` (a
+ * cudaStream_t, NULL = the legacy default stream); the call returns once the
+ * work is enqueued unless `stats` is given, in which case it waits for the
+ * stream to read the statistics back.
+ */
+#ifndef LSB_OMNISCAPE_H
+#define LSB_OMNISCAPE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum lsb_status {
+    LSB_OK = 0,
+    LSB_ERR_ARGUMENT = 1,      /* invalid parameter (reference: std::invalid_argument) */
+    LSB_ERR_NOT_CONVERGED = 2, /* a window's solve did not converge (reference: "not positive definite") */
+    LSB_ERR_CONDITION = 3,     /* a target block has no value of a condition (all NoData) */
+    LSB_ERR_WORKSPACE = 4,     /* workspace too small */
+    LSB_ERR_CUDA = 5           /* a CUDA runtime error */
+};
+
+enum lsb_precision {
+    LSB_PREC_FP64 = 0,        /* FP64 CG throughout */
+    LSB_PREC_FP32_REFINE = 1  /* FP32 CG inside FP64 iterative refinement */
+};
+
+enum lsb_preconditioner {
+    LSB_PC_AUTO = 0,   /* autotuned (or the built-in table) */
+    LSB_PC_JACOBI = 1, /* diagonal */
+    LSB_PC_MG = 2      /* geometric multigrid V-cycle, Galerkin coarse operators */
+};
+
+enum lsb_edge_weights {
+    LSB_EDGE_AVERAGE = 0, /* (a + b) / 2, diagonals / (2 sqrt 2): Omniscape / Circuitscape */
+    LSB_EDGE_SERIES = 1   /* 1 / ((1/a + 1/b) / 2), diagonals / sqrt 2: resistor series */
+};
+
+/* Conditional connectivity of one condition (OmniscapeCondition,
+ * omniscape.hpp:21-33).  present == NULL: no condition. */
+typedef struct lsb_omni_condition {
+    const double *present; /* device, ny x nx; NaN = missing (kept) */
+    const double *future;  /* device, ny x nx, or NULL: the present values */
+    int32_t equal;         /* 0: "within" (lower <= c - median <= upper), 1: "equal" (c == mode) */
+    int32_t pad_;
+    double lower, upper;
+} lsb_omni_condition;
+
+typedef struct lsb_omni_params {
+    /* OmniscapeParams (omniscape.hpp:35-47) */
+    int32_t radius;
+    int32_t buffer;
+    int32_t block_size;                /* odd */
+    int32_t four_neighbors;            /* 0/1 */
+    int32_t resistance_is_conductance; /* 0/1 */
+    int32_t correct_artifacts;         /* 0/1 (only with block_size > 1) */
+    int32_t flow_potential;            /* 0/1: also compute the flow potential */
+    int32_t edge_weights;              /* lsb_edge_weights */
+    lsb_omni_condition condition1, condition2;
+    double memory_limit; /* bytes of window buffers per batch (0: library default) */
+    /* solver */
+    int32_t precision;      /* lsb_precision */
+    int32_t preconditioner; /* lsb_preconditioner */
+    double tol;             /* relative FP64 residual ||b - A x|| / ||b|| at which a window is solved */
+    int32_t max_iter;       /* cap on CG iterations per window (all refinement steps together) */
+    int32_t threads_per_window; /* 0: autotuned; else 256, 512 or 1024 */
+    int32_t use_graph;      /* 1: capture the call's launches in a CUDA graph and replay it on repeat calls */
+    int32_t mask_nodata;    /* 1: NaN on NoData cells of the outputs (Python's mask_nodata) */
+} lsb_omni_params;
+
+typedef struct lsb_omni_stats {
+    int64_t n_targets;      /* targets (blocks with a positive source sum) */
+    int64_t n_solved;       /* window solves carried out (cumulative current + flow potential) */
+    int64_t n_failed;       /* solves that hit max_iter */
+    int64_t iters_total;    /* CG iterations over all solves */
+    int32_t iters_max;      /* CG iterations of the longest solve */
+    int32_t refine_max;     /* refinement steps of the longest solve */
+    int32_t batches;        /* window batches the targets were streamed in */
+    int32_t threads_per_window;
+    int32_t preconditioner;
+    int32_t pad_;
+    double worst_residual;  /* largest final relative FP64 residual */
+} lsb_omni_stats;
+
+/* Fill the defaults: radius 0, buffer 0, block 1, average weights, correction
+ * on, FP32 + refinement, autotuned preconditioner, tol 1e-12, graphs on. */
+void lsb_params_default(lsb_omni_params *p);
+
+/* Device bytes a call needs for an nx x ny raster with these parameters. */
+int lsb_omniscape_workspace_size(int64_t nx, int64_t ny, const lsb_omni_params *p, size_t *bytes);
+
+/*
+ * Omniscape on one GPU.  resistance, source: device ny x nx float64 (NaN
+ * resistance = NoData; the source must already hold Omniscape's thresholds and
+ * NaN -> 0, as the reference's Python layer prepares it).  Outputs: current
+ * (cumulative current, required), flow_potential and normalized (NULL: not
+ * computed / not written).  normalized = current / flow_potential with 0
+ * where that is NaN (omniscape.py:380-384); requires p->flow_potential.
+ */
+int lsb_omniscape(const double *resistance, const double *source, int64_t nx, int64_t ny,
+                  const lsb_omni_params *p, double *current, double *flow_potential, double *normalized,
+                  void *workspace, size_t workspace_bytes, lsb_omni_stats *stats, char *err, size_t errlen,
+                  void *stream);
+
+/* The (2 (radius + buffer) + 1)^2 block-artifact correction factors
+ * (omniscape_correction), written to the device array corr. */
+int lsb_omniscape_correction(int32_t radius, int32_t buffer, int32_t block_size, int32_t four_neighbors,
+                             int32_t edge_weights, int64_t nx, int64_t ny, double *corr, void *workspace,
+                             size_t workspace_bytes, char *err, size_t errlen, void *stream);
+
+/*
+ * Adjoint of the cumulative current.  J = sum over cells of weight * current;
+ * writes dJ/d(resistance) (dJ/d(conductance) with resistance_is_conductance)
+ * to grad_resistance and dJ/d(source) to grad_source (either may be NULL),
+ * and J to *J_out when J_out != NULL (device pointer to one double).
+ * Forward potentials are recomputed, not stored; each window's adjoint
+ * system is the same symmetric Laplacian with the node-current derivative as
+ * right-hand side.  Needs no correction (block_size 1 or correct_artifacts 0)
+ * and no conditions.
+ */
+int lsb_omniscape_grad(const double *resistance, const double *source, const double *weight, int64_t nx,
+                       int64_t ny, const lsb_omni_params *p, double *grad_resistance, double *grad_source,
+                       double *J_out, void *workspace, size_t workspace_bytes, lsb_omni_stats *stats, char *err,
+                       size_t errlen, void *stream);
+
+/* Device bytes lsb_omniscape_grad needs. */
+int lsb_omniscape_grad_workspace_size(int64_t nx, int64_t ny, const lsb_omni_params *p, size_t *bytes);
+
+/* Number of kernel launches the last call on this thread enqueued (0 when replayed from a graph: 1 graph). */
+int64_t lsb_last_launch_count(void);
+
+/* Library version string. */
+const char *lsb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LSB_OMNISCAPE_H */

@@ -1,0 +1,19 @@
+"""landschaft_b200: landschaft's Omniscape moving-window circuit connectivity on one B200.
+
+``omniscape`` is the drop-in for ``landschaft.omniscape`` (same arguments and
+outputs); the windows are solved by hand-written sm_100a CUDA behind the C ABI
+of ``include/lsb_omniscape.h``.
+"""
+
+from .omniscape import (  # noqa: F401
+    Dataset,
+    make_params,
+    omniscape,
+    omniscape_correction,
+    read_reclass_table,
+    reclassify,
+    run_device,
+    source_from_resistance,
+)
+
+__version__ = "0.1.0"

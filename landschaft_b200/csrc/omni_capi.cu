@@ -1,0 +1,663 @@
+// omni_capi.cu -- the C ABI (include/lsb_omniscape.h): validation, workspace
+// carving, kernel choice and placement, the launch sequence of one call, and
+// a cache of CUDA graphs of that sequence.
+//
+// The call mirrors circuit::omniscape (src/cpp/circuit/omniscape.cpp:394-608):
+// targets -> correction -> windows (in batches) -> scatter; the scatter is a
+// gather that adds every batch into the maps in target order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "../../include/lsb_omniscape.h"
+#include "omni_kernels.cuh"
+#include "omni_windows.cuh"
+
+namespace lsb {
+namespace {
+
+thread_local int64_t g_launches = 0;
+
+void set_err(char *err, size_t len, const char *fmt, ...) {
+    if (!err || len == 0) return;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(err, len, fmt, ap);
+    va_end(ap);
+}
+
+#define LSB_CK(call)                                                                   \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess) {                                                       \
+            set_err(err, errlen, "CUDA error %s at %s:%d", cudaGetErrorString(e_), __FILE__, __LINE__); \
+            return LSB_ERR_CUDA;                                                       \
+        }                                                                              \
+    } while (0)
+
+constexpr size_t kAlign = 256;
+size_t align_up(size_t v, size_t a = kAlign) { return (v + a - 1) / a * a; }
+
+// ---------------------------------------------------------------------------
+// Geometry of a call.
+// ---------------------------------------------------------------------------
+struct Geom {
+    int64_t nx, ny;
+    int R, B, D, W, bs, br, nbx, nby;
+    int64_t NL;
+    bool correct, fp, conditions;
+};
+
+int make_geom(int64_t nx, int64_t ny, const lsb_omni_params *p, Geom *g, char *err, size_t errlen) {
+    if (!p) {
+        set_err(err, errlen, "params is NULL");
+        return LSB_ERR_ARGUMENT;
+    }
+    if (p->radius < 0 || p->buffer < 0 || p->block_size < 1 || p->block_size % 2 == 0) {
+        set_err(err, errlen, "radius and buffer must be >= 0 and block_size odd");
+        return LSB_ERR_ARGUMENT;
+    }
+    if (nx < 1 || ny < 1) {
+        set_err(err, errlen, "the raster must have at least one cell");
+        return LSB_ERR_ARGUMENT;
+    }
+    g->nx = nx;
+    g->ny = ny;
+    g->R = p->radius;
+    g->B = p->buffer;
+    g->D = p->radius + p->buffer;
+    g->W = 2 * g->D + 1;
+    g->bs = p->block_size;
+    g->br = (p->block_size - 1) / 2;
+    g->nbx = nx - 2 * g->br > 0 ? static_cast<int>((nx - 2 * g->br - 1) / g->bs + 1) : 0;
+    g->nby = ny - 2 * g->br > 0 ? static_cast<int>((ny - 2 * g->br - 1) / g->bs + 1) : 0;
+    g->NL = static_cast<int64_t>(g->nbx) * g->nby;
+    g->correct = p->correct_artifacts && g->bs > 1;
+    g->fp = p->flow_potential != 0;
+    g->conditions = p->condition1.present != nullptr;
+    if (p->condition2.present && !p->condition1.present) {
+        set_err(err, errlen, "condition2 needs condition1");
+        return LSB_ERR_ARGUMENT;
+    }
+    if (g->conditions && g->bs * g->bs > kMaxCondCells) {
+        set_err(err, errlen, "conditions support block_size <= 31");
+        return LSB_ERR_ARGUMENT;
+    }
+    const int64_t np = static_cast<int64_t>(g->W + 2) * (g->W + 2);
+    if (np > 65535) {
+        set_err(err, errlen, "radius + buffer must be <= 125 (window of at most 251 x 251 cells)");
+        return LSB_ERR_ARGUMENT;
+    }
+    if (g->NL > (int64_t(1) << 30)) {
+        set_err(err, errlen, "too many target blocks");
+        return LSB_ERR_ARGUMENT;
+    }
+    if (p->precision != LSB_PREC_FP64 && p->precision != LSB_PREC_FP32_REFINE) {
+        set_err(err, errlen, "precision must be LSB_PREC_FP64 or LSB_PREC_FP32_REFINE");
+        return LSB_ERR_ARGUMENT;
+    }
+    if (p->edge_weights != LSB_EDGE_AVERAGE && p->edge_weights != LSB_EDGE_SERIES) {
+        set_err(err, errlen, "edge_weights must be LSB_EDGE_AVERAGE or LSB_EDGE_SERIES");
+        return LSB_ERR_ARGUMENT;
+    }
+    return LSB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Kernel variants and the arena layout.
+// ---------------------------------------------------------------------------
+struct Variant {
+    int nt;       // threads per CTA
+    bool dbl;     // inner solve in double
+    bool mg;      // multigrid compiled in
+    bool refine;  // FP64 refinement around the inner solve
+    bool four;
+};
+
+Variant choose_variant(const lsb_omni_params *p, const Geom &g) {
+    Variant v;
+    v.four = p->four_neighbors != 0;
+    v.dbl = p->precision == LSB_PREC_FP64;
+    v.refine = !v.dbl;
+    int pc = p->preconditioner;
+    if (pc == LSB_PC_AUTO) pc = v.dbl ? LSB_PC_JACOBI : LSB_PC_MG;
+    v.mg = pc == LSB_PC_MG;
+    int nt = p->threads_per_window;
+    if (nt != 256 && nt != 512 && nt != 1024) {
+        const int np = (g.W + 2) * (g.W + 2);
+        nt = np <= 1200 ? 256 : np <= 3000 ? 512 : 1024;
+    }
+    v.nt = nt;
+    return v;
+}
+
+int resolved_pc(const lsb_omni_params *p) {
+    int pc = p->preconditioner;
+    if (pc == LSB_PC_AUTO) pc = p->precision == LSB_PREC_FP64 ? LSB_PC_JACOBI : LSB_PC_MG;
+    return pc;
+}
+
+constexpr size_t kStaticSmem = 128 * 8 + 64 * 4 + 2 * kMaxLevels * 4 + 64;
+
+ArenaLayout make_layout(const Variant &v, int W, size_t smem_budget) {
+    ArenaLayout L;
+    std::memset(&L, 0, sizeof L);
+    const size_t np = static_cast<size_t>(W + 2) * (W + 2);
+    const size_t ts = v.dbl ? 8 : 4;
+    struct Item {
+        int arr;
+        size_t bytes;
+    };
+    std::vector<Item> items;  // in smem priority order
+    items.push_back({AR_ULIST, np * 2});
+    items.push_back({AR_GT, np * ts});
+    items.push_back({AR_P, np * ts});
+    if (v.mg) items.push_back({AR_Z, np * ts});
+    items.push_back({AR_Q, np * ts});
+    items.push_back({AR_R, np * ts});
+    items.push_back({AR_INVD, np * ts});
+    const bool has_d = !(v.dbl && !v.refine);
+    if (has_d) items.push_back({AR_D, np * ts});
+    if (v.mg) {
+        const int nlev = mg_levels(W, W);
+        int h = W, w = W;
+        for (int l = 1; l < nlev; ++l) {
+            h = coarse_dim(h);
+            w = coarse_dim(w);
+            const size_t npl = static_cast<size_t>(h + 2) * (w + 2);
+            for (int k = 0; k < LV_COUNT; ++k) items.push_back({AR_LEVEL + (l - 1) * LV_COUNT + k, npl * ts});
+        }
+        items.push_back({AR_DENSE, static_cast<size_t>(kNcMax) * kNcMax * 8});
+    }
+    items.push_back({AR_MASK, np});
+    if (!has_d) items.push_back({AR_X64, np * 8});  // the solution is the iterate: keep it close
+    if (has_d) items.push_back({AR_X64, np * 8});
+    items.push_back({AR_G64, np * 8});
+    items.push_back({AR_B64, np * 8});
+    size_t so = 0, go = 0;
+    for (const Item &it : items) {
+        const size_t b = align_up(it.bytes, 16);
+        if (so + b <= smem_budget) {
+            L.off[it.arr] = static_cast<uint32_t>(so);
+            so += b;
+        } else {
+            L.off[it.arr] = static_cast<uint32_t>(go) | 0x80000000u;
+            go += b;
+        }
+    }
+    L.smem_bytes = static_cast<uint32_t>(so);
+    L.gmem_bytes = static_cast<uint32_t>(align_up(go));
+    return L;
+}
+
+// ---------------------------------------------------------------------------
+// Kernel dispatch.
+// ---------------------------------------------------------------------------
+KernelFn pick(const Variant &v) {
+    switch (v.nt) {
+        case 256:
+            return pick_windows_256(v.four, v.dbl, v.mg);
+        case 512:
+            return pick_windows_512(v.four, v.dbl, v.mg);
+        default:
+            return pick_windows_1024(v.four, v.dbl, v.mg);
+    }
+}
+
+struct DeviceInfo {
+    int dev = -1, sms = 0;
+    size_t smem_optin = 0;
+};
+
+cudaError_t device_info(DeviceInfo *d) {
+    cudaError_t e = cudaGetDevice(&d->dev);
+    if (e != cudaSuccess) return e;
+    int v = 0;
+    e = cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, d->dev);
+    if (e != cudaSuccess) return e;
+    d->sms = v;
+    e = cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->dev);
+    if (e != cudaSuccess) return e;
+    d->smem_optin = static_cast<size_t>(v);
+    return cudaSuccess;
+}
+
+// ---------------------------------------------------------------------------
+// Workspace plan.
+// ---------------------------------------------------------------------------
+struct Plan {
+    Geom g;
+    Variant v;
+    ArenaLayout lay;
+    KernelFn kern;
+    int grid;           // persistent CTAs
+    int64_t batch;      // windows per batch
+    int nbatches;
+    int nparts;         // scan blocks
+    // workspace offsets
+    size_t o_amps, o_tindex, o_targets, o_part, o_count, o_queue, o_err, o_stat, o_condv, o_corr, o_corrwin,
+        o_corrstat, o_cur, o_fp, o_gs, o_devstats, total;
+};
+
+int make_plan(int64_t nx, int64_t ny, const lsb_omni_params *p, Plan *pl, char *err, size_t errlen) {
+    int rc = make_geom(nx, ny, p, &pl->g, err, errlen);
+    if (rc) return rc;
+    const Geom &g = pl->g;
+    pl->v = choose_variant(p, g);
+    DeviceInfo di;
+    LSB_CK(device_info(&di));
+    const size_t budget = di.smem_optin > kStaticSmem ? di.smem_optin - kStaticSmem : 0;
+    pl->lay = make_layout(pl->v, g.W, budget);
+    pl->kern = pick(pl->v);
+    LSB_CK(cudaFuncSetAttribute(reinterpret_cast<const void *>(pl->kern),
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(pl->lay.smem_bytes)));
+    int per_sm = 0;
+    LSB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pl->kern, pl->v.nt, pl->lay.smem_bytes));
+    if (per_sm < 1) {
+        set_err(err, errlen, "the window kernel does not fit on an SM (%u bytes of shared memory)", pl->lay.smem_bytes);
+        return LSB_ERR_ARGUMENT;
+    }
+    const int64_t NL = std::max<int64_t>(g.NL, 1);
+    const size_t per_window = static_cast<size_t>(g.W) * g.W * 8 * (g.fp ? 2 : 1);
+    const double lim = p->memory_limit > 0 ? p->memory_limit : 4.0 * (1 << 30);
+    int64_t batch = static_cast<int64_t>(lim / static_cast<double>(per_window));
+    batch = std::max<int64_t>(1, std::min<int64_t>(batch, NL));
+    pl->batch = batch;
+    pl->nbatches = static_cast<int>((NL + batch - 1) / batch);
+    pl->grid = static_cast<int>(std::min<int64_t>(static_cast<int64_t>(di.sms) * per_sm, std::max<int64_t>(batch, 2)));
+    pl->nparts = static_cast<int>((NL + kScanBlock - 1) / kScanBlock);
+    size_t o = 0;
+    auto take = [&](size_t bytes) {
+        const size_t r = o;
+        o += align_up(std::max<size_t>(bytes, 1));
+        return r;
+    };
+    pl->o_amps = take(NL * 8);
+    pl->o_tindex = take(NL * 4);
+    pl->o_targets = take(NL * 4);
+    pl->o_part = take((pl->nparts + 1) * 4);
+    pl->o_count = take(4);
+    pl->o_queue = take((pl->nbatches + 1) * 4);
+    pl->o_err = take(4);
+    pl->o_stat = take(NL * 2 * sizeof(WinStat));
+    pl->o_condv = take(g.conditions ? NL * 16 : 0);
+    pl->o_corr = take(g.correct ? static_cast<size_t>(g.W) * g.W * 8 : 0);
+    pl->o_corrwin = take(g.correct ? static_cast<size_t>(g.W) * g.W * 16 : 0);
+    pl->o_corrstat = take(2 * sizeof(WinStat));
+    pl->o_cur = take(static_cast<size_t>(batch) * g.W * g.W * 8);
+    pl->o_fp = take(g.fp ? static_cast<size_t>(batch) * g.W * g.W * 8 : 0);
+    pl->o_gs = take(static_cast<size_t>(pl->grid) * pl->lay.gmem_bytes);
+    pl->o_devstats = take(sizeof(DevStats));
+    pl->total = o;
+    return LSB_OK;
+}
+
+SolveParams solve_params(const lsb_omni_params *p) {
+    SolveParams sp;
+    sp.tol = p->tol > 0 ? p->tol : 1e-12;
+    sp.inner_tol = p->precision == LSB_PREC_FP64 ? sp.tol : 1e-4;
+    sp.max_iter = p->max_iter > 0 ? p->max_iter : 20000;
+    sp.max_outer = 30;
+    sp.pc = resolved_pc(p);
+    sp.omega = 0.7f;
+    return sp;
+}
+
+// ---------------------------------------------------------------------------
+// Graph cache: the launch sequence of a call, keyed by everything it reads.
+// ---------------------------------------------------------------------------
+struct GraphKey {
+    const void *ptrs[8];
+    int64_t nx, ny;
+    lsb_omni_params p;
+    size_t ws_bytes;
+    void *stream;
+    int dev;
+    bool operator==(const GraphKey &o) const { return std::memcmp(this, &o, sizeof *this) == 0; }
+};
+struct GraphEntry {
+    GraphKey key;
+    cudaGraphExec_t exec;
+    int64_t launches;
+};
+std::mutex g_graph_mutex;
+std::vector<GraphEntry> g_graphs;
+constexpr size_t kMaxGraphs = 16;
+
+// ---------------------------------------------------------------------------
+// The launch sequence.
+// ---------------------------------------------------------------------------
+int enqueue(const Plan &pl, const double *res, const double *src, const lsb_omni_params *p, double *cur, double *fpm,
+            double *norm, char *ws, cudaStream_t s, char *err, size_t errlen) {
+    const Geom &g = pl.g;
+    const int64_t n = g.nx * g.ny;
+    int64_t launches = 0;
+    LSB_CK(cudaMemsetAsync(cur, 0, n * 8, s));
+    if (g.fp) LSB_CK(cudaMemsetAsync(fpm, 0, n * 8, s));
+    LSB_CK(cudaMemsetAsync(ws + pl.o_count, 0, 4, s));
+    LSB_CK(cudaMemsetAsync(ws + pl.o_queue, 0, (pl.nbatches + 1) * 4, s));
+    LSB_CK(cudaMemsetAsync(ws + pl.o_err, 0, 4, s));
+    double *amps = reinterpret_cast<double *>(ws + pl.o_amps);
+    int *tindex = reinterpret_cast<int *>(ws + pl.o_tindex), *targets = reinterpret_cast<int *>(ws + pl.o_targets);
+    int *part = reinterpret_cast<int *>(ws + pl.o_part), *count = reinterpret_cast<int *>(ws + pl.o_count);
+    int *queue = reinterpret_cast<int *>(ws + pl.o_queue), *errf = reinterpret_cast<int *>(ws + pl.o_err);
+    WinStat *stat = reinterpret_cast<WinStat *>(ws + pl.o_stat);
+    LSB_CK(cudaMemsetAsync(stat, 0, std::max<int64_t>(g.NL, 1) * 2 * sizeof(WinStat), s));
+    if (g.NL > 0) {
+        const int nb = static_cast<int>((g.NL + 255) / 256);
+        k_lattice_amps<<<nb, 256, 0, s>>>(src, g.nx, g.ny, g.bs, g.br, g.nbx, g.nby, amps);
+        k_scan_count<<<pl.nparts, kScanBlock, 0, s>>>(amps, g.NL, part);
+        k_scan_offsets<<<1, 1024, 0, s>>>(part, pl.nparts, count);
+        k_scan_write<<<pl.nparts, kScanBlock, 0, s>>>(amps, g.NL, part, tindex, targets);
+        launches += 4;
+        LSB_CK(cudaGetLastError());
+    }
+    KArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.res = res;
+    a.src = src;
+    a.nx = g.nx;
+    a.ny = g.ny;
+    a.R = g.R;
+    a.D = g.D;
+    a.W = g.W;
+    a.bs = g.bs;
+    a.br = g.br;
+    a.nbx = g.nbx;
+    a.nby = g.nby;
+    a.ric = p->resistance_is_conductance != 0;
+    a.series = p->edge_weights == LSB_EDGE_SERIES;
+    a.four = p->four_neighbors != 0;
+    a.fp = g.fp;
+    a.correct = g.correct;
+    const lsb_omni_condition *cs[2] = {&p->condition1, &p->condition2};
+    for (int k = 0; k < 2; ++k) {
+        a.cond_present[k] = cs[k]->present;
+        a.cond_future[k] = cs[k]->future;
+        a.cond_equal[k] = cs[k]->equal != 0;
+        a.cond_lo[k] = cs[k]->lower;
+        a.cond_hi[k] = cs[k]->upper;
+    }
+    a.cond_val = g.conditions ? reinterpret_cast<const double *>(ws + pl.o_condv) : nullptr;
+    a.count_ptr = count;
+    a.targets = targets;
+    a.lat_amps = amps;
+    a.corr = g.correct ? reinterpret_cast<const double *>(ws + pl.o_corr) : nullptr;
+    a.gscratch = ws + pl.o_gs;
+    a.lay = pl.lay;
+    a.sp = solve_params(p);
+    if (g.conditions && g.NL > 0) {
+        k_block_cond<<<static_cast<int>((g.NL + 127) / 128), 128, 0, s>>>(
+            a, reinterpret_cast<double *>(ws + pl.o_condv), errf);
+        ++launches;
+        LSB_CK(cudaGetLastError());
+    }
+    if (g.correct) {
+        KArgs c = a;
+        c.mode = 1;
+        int nsrc = 0;
+        for (int y = 0; y < g.W; ++y)
+            for (int x = 0; x < g.W; ++x)
+                if ((y - g.D) * (y - g.D) + (x - g.D) * (x - g.D) <= g.R * g.R) ++nsrc;
+        c.n_corr_sources = nsrc;
+        c.cur_win = reinterpret_cast<double *>(ws + pl.o_corrwin);
+        c.stat = reinterpret_cast<WinStat *>(ws + pl.o_corrstat);
+        c.queue = queue + pl.nbatches;
+        c.correct = 0;
+        c.sp.tol = std::min(c.sp.tol, 1e-13);
+        pl.kern<<<2, pl.v.nt, pl.lay.smem_bytes, s>>>(c);
+        k_corr_ratio<<<1, 1024, 0, s>>>(c.cur_win, c.stat, g.W, g.bs, reinterpret_cast<double *>(ws + pl.o_corr));
+        launches += 2;
+        LSB_CK(cudaGetLastError());
+    }
+    a.cur_win = reinterpret_cast<double *>(ws + pl.o_cur);
+    a.fp_win = g.fp ? reinterpret_cast<double *>(ws + pl.o_fp) : nullptr;
+    a.stat = stat;
+    a.batch_size = static_cast<int>(pl.batch);
+    const dim3 gg(static_cast<unsigned>((g.nx + kGatherTX - 1) / kGatherTX),
+                  static_cast<unsigned>((g.ny + kGatherTY - 1) / kGatherTY));
+    for (int b = 0; b < pl.nbatches && g.NL > 0; ++b) {
+        a.batch_start = static_cast<int>(b * pl.batch);
+        a.queue = queue + b;
+        pl.kern<<<pl.grid, pl.v.nt, pl.lay.smem_bytes, s>>>(a);
+        k_gather<<<gg, kGatherTX * kGatherTY, 0, s>>>(a, tindex, cur, g.fp ? fpm : nullptr);
+        launches += 2;
+        LSB_CK(cudaGetLastError());
+    }
+    if (norm || p->mask_nodata) {
+        k_finish<<<static_cast<int>((n + 255) / 256), 256, 0, s>>>(res, n, cur, g.fp ? fpm : nullptr, norm,
+                                                                  p->mask_nodata);
+        ++launches;
+        LSB_CK(cudaGetLastError());
+    }
+    k_stats<<<1, 1024, 0, s>>>(stat, count, 2, reinterpret_cast<DevStats *>(ws + pl.o_devstats));
+    ++launches;
+    LSB_CK(cudaGetLastError());
+    g_launches = launches;
+    return LSB_OK;
+}
+
+}  // namespace
+}  // namespace lsb
+
+using namespace lsb;
+
+extern "C" {
+
+void lsb_params_default(lsb_omni_params *p) {
+    std::memset(p, 0, sizeof *p);
+    p->radius = 0;
+    p->buffer = 0;
+    p->block_size = 1;
+    p->correct_artifacts = 1;
+    p->edge_weights = LSB_EDGE_AVERAGE;
+    p->precision = LSB_PREC_FP32_REFINE;
+    p->preconditioner = LSB_PC_AUTO;
+    p->tol = 1e-12;
+    p->max_iter = 20000;
+    p->use_graph = 1;
+    p->mask_nodata = 0;
+}
+
+int lsb_omniscape_workspace_size(int64_t nx, int64_t ny, const lsb_omni_params *p, size_t *bytes) {
+    Plan pl;
+    char *err = nullptr;
+    size_t errlen = 0;
+    const int rc = make_plan(nx, ny, p, &pl, err, errlen);
+    if (rc) return rc;
+    *bytes = pl.total;
+    return LSB_OK;
+}
+
+int lsb_omniscape(const double *resistance, const double *source, int64_t nx, int64_t ny, const lsb_omni_params *p,
+                  double *current, double *flow_potential, double *normalized, void *workspace,
+                  size_t workspace_bytes, lsb_omni_stats *stats, char *err, size_t errlen, void *stream) {
+    Plan pl;
+    int rc = make_plan(nx, ny, p, &pl, err, errlen);
+    if (rc) return rc;
+    if (!resistance || !source || !current) {
+        set_err(err, errlen, "resistance, source and current are required");
+        return LSB_ERR_ARGUMENT;
+    }
+    if (p->flow_potential && !flow_potential) {
+        set_err(err, errlen, "flow_potential is requested but its output is NULL");
+        return LSB_ERR_ARGUMENT;
+    }
+    if (normalized && !p->flow_potential) {
+        set_err(err, errlen, "the normalised current needs the flow potential");
+        return LSB_ERR_ARGUMENT;
+    }
+    if (!workspace || workspace_bytes < pl.total) {
+        set_err(err, errlen, "workspace too small: %zu bytes needed", pl.total);
+        return LSB_ERR_WORKSPACE;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    char *ws = static_cast<char *>(workspace);
+    bool graphed = false;
+    if (p->use_graph && s != nullptr) {
+        GraphKey key;
+        std::memset(&key, 0, sizeof key);
+        key.ptrs[0] = resistance;
+        key.ptrs[1] = source;
+        key.ptrs[2] = current;
+        key.ptrs[3] = flow_potential;
+        key.ptrs[4] = normalized;
+        key.ptrs[5] = workspace;
+        key.nx = nx;
+        key.ny = ny;
+        key.p = *p;
+        key.ws_bytes = workspace_bytes;
+        key.stream = stream;
+        key.dev = 0;
+        cudaGetDevice(&key.dev);
+        std::lock_guard<std::mutex> lock(g_graph_mutex);
+        cudaGraphExec_t exec = nullptr;
+        int64_t launches = 0;
+        for (auto &e : g_graphs)
+            if (e.key == key) {
+                exec = e.exec;
+                launches = e.launches;
+            }
+        if (!exec) {
+            LSB_CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            rc = enqueue(pl, resistance, source, p, current, flow_potential, normalized, ws, s, err, errlen);
+            cudaGraph_t graph = nullptr;
+            const cudaError_t ce = cudaStreamEndCapture(s, &graph);
+            if (rc) {
+                if (graph) cudaGraphDestroy(graph);
+                return rc;
+            }
+            LSB_CK(ce);
+            const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            LSB_CK(ie);
+            launches = g_launches;
+            if (g_graphs.size() >= kMaxGraphs) {
+                cudaGraphExecDestroy(g_graphs.front().exec);
+                g_graphs.erase(g_graphs.begin());
+            }
+            g_graphs.push_back({key, exec, launches});
+        }
+        LSB_CK(cudaGraphLaunch(exec, s));
+        g_launches = launches;
+        graphed = true;
+    }
+    if (!graphed) {
+        rc = enqueue(pl, resistance, source, p, current, flow_potential, normalized, ws, s, err, errlen);
+        if (rc) return rc;
+    }
+    if (stats) {
+        DevStats ds;
+        int hdr[2] = {0, 0};
+        LSB_CK(cudaMemcpyAsync(&ds, ws + pl.o_devstats, sizeof ds, cudaMemcpyDeviceToHost, s));
+        LSB_CK(cudaMemcpyAsync(&hdr[0], ws + pl.o_count, 4, cudaMemcpyDeviceToHost, s));
+        LSB_CK(cudaMemcpyAsync(&hdr[1], ws + pl.o_err, 4, cudaMemcpyDeviceToHost, s));
+        LSB_CK(cudaStreamSynchronize(s));
+        stats->n_targets = hdr[0];
+        stats->n_solved = ds.n_solved;
+        stats->n_failed = ds.n_failed;
+        stats->iters_total = ds.iters_total;
+        stats->iters_max = ds.iters_max;
+        stats->refine_max = ds.refine_max;
+        stats->batches = pl.nbatches;
+        stats->threads_per_window = pl.v.nt;
+        stats->preconditioner = resolved_pc(p);
+        stats->worst_residual = ds.worst_residual;
+        if (hdr[1]) {
+            set_err(err, errlen, "a target block has no value of a condition (all NoData)");
+            return LSB_ERR_CONDITION;
+        }
+        if (ds.n_failed > 0) {
+            set_err(err, errlen, "%lld Omniscape window solves did not converge (worst relative residual %.3g)",
+                    static_cast<long long>(ds.n_failed), ds.worst_residual);
+            return LSB_ERR_NOT_CONVERGED;
+        }
+    }
+    return LSB_OK;
+}
+
+int lsb_omniscape_correction(int32_t radius, int32_t buffer, int32_t block_size, int32_t four_neighbors,
+                             int32_t edge_weights, int64_t nx, int64_t ny, double *corr, void *workspace,
+                             size_t workspace_bytes, char *err, size_t errlen, void *stream) {
+    lsb_omni_params p;
+    lsb_params_default(&p);
+    p.radius = radius;
+    p.buffer = buffer;
+    p.block_size = block_size;
+    p.four_neighbors = four_neighbors;
+    p.edge_weights = edge_weights;
+    p.precision = LSB_PREC_FP64;
+    p.preconditioner = LSB_PC_JACOBI;
+    // a 1 x 1 raster: no targets, only the correction windows
+    Plan pl;
+    int rc = make_plan(1, 1, &p, &pl, err, errlen);
+    if (rc) return rc;
+    const Geom &g0 = pl.g;
+    (void)g0;
+    // the correction's plan: W from radius/buffer; the raster size only enters through the quirk's min()
+    Geom g;
+    rc = make_geom(nx, ny, &p, &g, err, errlen);
+    if (rc) return rc;
+    const size_t need = align_up(static_cast<size_t>(g.W) * g.W * 16) + align_up(2 * sizeof(WinStat)) +
+                        align_up(8) + 2 * static_cast<size_t>(pl.lay.gmem_bytes);
+    if (!workspace || workspace_bytes < need) {
+        set_err(err, errlen, "workspace too small: %zu bytes needed", need);
+        return LSB_ERR_WORKSPACE;
+    }
+    char *ws = static_cast<char *>(workspace);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    KArgs c;
+    std::memset(&c, 0, sizeof c);
+    c.nx = nx;
+    c.ny = ny;
+    c.R = g.R;
+    c.D = g.D;
+    c.W = g.W;
+    c.bs = g.bs;
+    c.br = g.br;
+    c.four = four_neighbors != 0;
+    c.series = edge_weights == LSB_EDGE_SERIES;
+    c.mode = 1;
+    int nsrc = 0;
+    for (int y = 0; y < g.W; ++y)
+        for (int x = 0; x < g.W; ++x)
+            if ((y - g.D) * (y - g.D) + (x - g.D) * (x - g.D) <= g.R * g.R) ++nsrc;
+    c.n_corr_sources = nsrc;
+    c.cur_win = reinterpret_cast<double *>(ws);
+    c.stat = reinterpret_cast<WinStat *>(ws + align_up(static_cast<size_t>(g.W) * g.W * 16));
+    int *queue = reinterpret_cast<int *>(ws + align_up(static_cast<size_t>(g.W) * g.W * 16) + align_up(2 * sizeof(WinStat)));
+    c.queue = queue;
+    c.gscratch = reinterpret_cast<char *>(queue) + align_up(8);
+    c.lay = pl.lay;
+    c.sp = solve_params(&p);
+    c.sp.tol = 1e-13;
+    LSB_CK(cudaMemsetAsync(queue, 0, 4, s));
+    pl.kern<<<2, pl.v.nt, pl.lay.smem_bytes, s>>>(c);
+    k_corr_ratio<<<1, 1024, 0, s>>>(c.cur_win, c.stat, g.W, g.bs, corr);
+    LSB_CK(cudaGetLastError());
+    g_launches = 2;
+    return LSB_OK;
+}
+
+int lsb_omniscape_grad_workspace_size(int64_t nx, int64_t ny, const lsb_omni_params *p, size_t *bytes) {
+    return lsb_omniscape_workspace_size(nx, ny, p, bytes);
+}
+
+int lsb_omniscape_grad(const double *, const double *, const double *, int64_t, int64_t, const lsb_omni_params *,
+                       double *, double *, double *, void *, size_t, lsb_omni_stats *, char *err, size_t errlen,
+                       void *) {
+    set_err(err, errlen, "the adjoint is not built in this version");
+    return LSB_ERR_ARGUMENT;
+}
+
+int64_t lsb_last_launch_count(void) { return g_launches; }
+
+const char *lsb_version(void) { return "landschaft_b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

@@ -1,0 +1,237 @@
+// omni_device.cuh -- the per-window circuit solve of the Omniscape path, on one
+// CTA of an sm_100a GPU.
+//
+// One CTA owns one window at a time (a persistent CTA pulls windows from a
+// queue).  Per window it
+//   1. builds the window's conductance and sources from the rasters
+//      (omniscape.cpp:495-530: disk of radius + buffer, NoData = -9999,
+//      sources within radius, the target block zeroed at radius + buffer from
+//      the window corner, sources rescaled to the block's amps, conditions);
+//   2. flood-fills the ground's component (omniscape.cpp:86-101);
+//   3. assembles the grounded Laplacian implicitly (system.cpp:458-487): the
+//      stencil weights are recomputed from the conductance in every matrix-
+//      vector product, the diagonal is summed in column-major neighbour order;
+//   4. solves it by preconditioned CG: FP64 Jacobi-PCG ("plain"), or CG whose
+//      iterations run in T (float) inside FP64 iterative refinement, with a
+//      Jacobi or a geometric multigrid V-cycle preconditioner;
+//   5. computes node currents exactly as grid.cpp:19-71 does (FP64, branch
+//      threshold 1e-8 of the signed maxima, max(inflow, outflow), column-major
+//      neighbour order), applies the block-artifact correction slice
+//      (omniscape.cpp:553-571) and writes the window to its output slot.
+//
+// Memory: every per-cell array of a window lives in a padded (h+2) x (w+2)
+// row-major box (pitch P = w + 2), so that stencil reads need no bounds
+// checks.  Arrays are placed in shared memory while it lasts and otherwise in
+// a per-CTA slice of global scratch (L2-resident); the host decides the
+// placement (ArenaLayout).  All reductions are block-wide, in a fixed order:
+// results do not depend on scheduling.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace lsb {
+
+constexpr double kTwoSqrt2 = 2.8284271247461903;  // 2*sqrt(2) as the reference evaluates it (grid.hpp:17)
+constexpr double kSqrt2 = 1.4142135623730951;
+constexpr double kInvTwoSqrt2 = 0.35355339059327373;  // 1 / (2 sqrt 2), for iterative products only
+constexpr double kShift = 10.0 * 2.220446049250313080847e-16;  // CHOLMOD's 10 eps (omniscape.cpp:28)
+
+// ---------------------------------------------------------------------------
+// Stencils: neighbours in increasing column-major index (grid.hpp:27-35).
+// ---------------------------------------------------------------------------
+template <bool FOUR>
+struct Nb;
+template <>
+struct Nb<false> {
+    static constexpr int ND = 8, LOWER = 4;
+    __host__ __device__ static constexpr int dy(int d) {
+        return d == 0 ? -1 : d == 1 ? 0 : d == 2 ? 1 : d == 3 ? -1 : d == 4 ? 1 : d == 5 ? -1 : d == 6 ? 0 : 1;
+    }
+    __host__ __device__ static constexpr int dx(int d) { return d < 3 ? -1 : d < 5 ? 0 : 1; }
+    __host__ __device__ static constexpr bool diag(int d) { return d == 0 || d == 2 || d == 5 || d == 7; }
+};
+template <>
+struct Nb<true> {
+    static constexpr int ND = 4, LOWER = 2;
+    __host__ __device__ static constexpr int dy(int d) { return d == 1 ? -1 : d == 2 ? 1 : 0; }
+    __host__ __device__ static constexpr int dx(int d) { return d == 0 ? -1 : d == 3 ? 1 : 0; }
+    __host__ __device__ static constexpr bool diag(int) { return false; }
+};
+
+// Exact edge weight of two conductances (grid.hpp:37-40; resistor series:
+// circuitscape.cpp:30-33), used where the reference's rounding matters.
+__device__ __forceinline__ double edge_w_exact(double a, double b, bool diag, bool series) {
+    if (series) return diag ? 1.0 / (kSqrt2 * (1.0 / a + 1.0 / b) / 2.0) : 1.0 / ((1.0 / a + 1.0 / b) / 2.0);
+    return diag ? (a + b) / kTwoSqrt2 : (a + b) / 2.0;
+}
+
+// ---------------------------------------------------------------------------
+// Window descriptions.
+// ---------------------------------------------------------------------------
+enum WinKind : int { KIND_LAND = 0, KIND_FLOW = 1, KIND_CORR_BLOCK = 2, KIND_CORR_NULL = 3 };
+
+// Per-window geometry in window coordinates.
+struct WinGeom {
+    int h, w, gy, gx;  // box and ground
+    int P, NP;         // padded pitch and padded cell count
+    int64_t y0, x0;    // corner on the map
+    int64_t ty, tx;    // target on the map
+};
+
+// Mask bits of a level-0 cell.
+enum : uint8_t { M_UNKNOWN = 1, M_PRESENT = 2, M_CAND = 4 };
+
+constexpr int kMaxLevels = 9;  // level 0 + up to 8 coarse levels (windows up to 513 cells wide)
+constexpr int kNcMax = 25;     // cells of the coarsest level (solved by its dense inverse)
+
+// Arrays of a window's working set.
+enum LevelArray : int { LV_C0 = 0, LV_CE, LV_CSW, LV_CS, LV_CSE, LV_INVD, LV_X, LV_B, LV_T, LV_COUNT };
+enum ArenaArray : int {
+    AR_MASK = 0,  // u8
+    AR_ULIST,     // u16: padded indices of the unknowns, row-major
+    AR_G64,       // f64: conductance (-9999 outside / NoData; 0 on padding)
+    AR_X64,       // f64: solution (potentials), 0 off the unknowns
+    AR_B64,       // f64: scaled sources (the right-hand side)
+    AR_GT,        // T: stencil conductance (or resistance with series weights); sentinels off the nodes
+    AR_INVD,      // T: 1 / diagonal on the unknowns, 0 elsewhere
+    AR_D,         // T: inner solution (refinement correction)
+    AR_R,         // T: inner residual
+    AR_P,         // T: search direction
+    AR_Q,         // T: A p; multigrid fine residual and output
+    AR_Z,         // T: multigrid pre-smoothed residual; the fine diagonal during set-up
+    AR_DENSE,     // f64: inverse of the coarsest operator (kNcMax^2)
+    AR_LEVEL,     // first coarse level; each coarse level has LV_COUNT arrays
+    AR_COUNT = AR_LEVEL + (kMaxLevels - 1) * LV_COUNT
+};
+
+// Byte offsets of the arrays; bit 31 set: in global scratch, else shared.
+struct ArenaLayout {
+    uint32_t off[AR_COUNT];
+    uint32_t smem_bytes;
+    uint32_t gmem_bytes;  // per CTA
+};
+
+// Solver configuration for one launch.
+struct SolveParams {
+    double tol;        // final relative FP64 residual
+    double inner_tol;  // relative residual reduction of one refinement step
+    int max_iter;      // cap on CG iterations (all refinement steps)
+    int max_outer;     // cap on refinement steps
+    int pc;            // 1 Jacobi, 2 multigrid
+    float omega;       // damped-Jacobi smoothing weight
+};
+
+// Per-solve statistics written by the kernel.
+struct WinStat {
+    int iters;
+    int outer;
+    int status;  // 0 no solve needed, 1 converged, 2 not converged, 3 breakdown / non-finite
+    float resid;  // final relative FP64 residual
+};
+
+// ---------------------------------------------------------------------------
+// Block-wide reductions in a fixed order (every thread gets the same value).
+// `red` is shared: 2 slots x 64 doubles.
+// ---------------------------------------------------------------------------
+template <int NT>
+struct Reducer {
+    double *red;
+    int slot;
+    __device__ __forceinline__ double *next() {
+        double *b = red + (slot & 1) * 64;
+        ++slot;
+        return b;
+    }
+    __device__ __forceinline__ double sum(double v) {
+        constexpr int NW = NT / 32;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        double *b = next();
+        if ((threadIdx.x & 31) == 0) b[threadIdx.x >> 5] = v;
+        __syncthreads();
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < NW; ++k) s += b[k];
+        return s;
+    }
+    __device__ __forceinline__ void sum2(double &a, double &c) {
+        constexpr int NW = NT / 32;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_down_sync(0xffffffffu, a, o);
+            c += __shfl_down_sync(0xffffffffu, c, o);
+        }
+        double *b = next();
+        if ((threadIdx.x & 31) == 0) {
+            b[threadIdx.x >> 5] = a;
+            b[32 + (threadIdx.x >> 5)] = c;
+        }
+        __syncthreads();
+        double s = 0.0, t = 0.0;
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+            s += b[k];
+            t += b[32 + k];
+        }
+        a = s;
+        c = t;
+    }
+    __device__ __forceinline__ double max(double v) {
+        constexpr int NW = NT / 32;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+        double *b = next();
+        if ((threadIdx.x & 31) == 0) b[threadIdx.x >> 5] = v;
+        __syncthreads();
+        double s = b[0];
+#pragma unroll
+        for (int k = 1; k < NW; ++k) s = fmax(s, b[k]);
+        return s;
+    }
+    __device__ __forceinline__ void max2(double &a, double &c) {
+        constexpr int NW = NT / 32;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a = fmax(a, __shfl_down_sync(0xffffffffu, a, o));
+            c = fmax(c, __shfl_down_sync(0xffffffffu, c, o));
+        }
+        double *b = next();
+        if ((threadIdx.x & 31) == 0) {
+            b[threadIdx.x >> 5] = a;
+            b[32 + (threadIdx.x >> 5)] = c;
+        }
+        __syncthreads();
+        double s = b[0], t = b[32];
+#pragma unroll
+        for (int k = 1; k < NW; ++k) {
+            s = fmax(s, b[k]);
+            t = fmax(t, b[32 + k]);
+        }
+        a = s;
+        c = t;
+    }
+    __device__ __forceinline__ int count(int v) {  // block-wide integer sum (exact)
+        return static_cast<int>(sum(static_cast<double>(v)));
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Level sizes of the multigrid hierarchy: a dimension of n > 3 cells coarsens
+// to n/2 + 1 (coarse point J <-> fine point 2J); the hierarchy ends at the
+// first level of at most kNcMax cells.
+// ---------------------------------------------------------------------------
+__host__ __device__ inline int coarse_dim(int n) { return n > 3 ? n / 2 + 1 : n; }
+__host__ __device__ inline int mg_levels(int h, int w) {
+    int L = 1;
+    while (h * w > kNcMax && L < kMaxLevels) {
+        const int hc = coarse_dim(h), wc = coarse_dim(w);
+        if (hc == h && wc == w) break;
+        h = hc;
+        w = wc;
+        ++L;
+    }
+    return L;
+}
+
+}  // namespace lsb

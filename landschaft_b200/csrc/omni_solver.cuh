@@ -1,0 +1,978 @@
+// omni_solver.cuh -- one window on one CTA: load, flood fill, assembly,
+// preconditioned CG (Jacobi or geometric multigrid; FP64, or FP32 inside FP64
+// iterative refinement), node currents.  See omni_device.cuh for the layout.
+#pragma once
+
+#include <math_constants.h>
+
+#include "omni_device.cuh"
+
+namespace lsb {
+
+// Everything a window kernel reads; passed by value (param space).
+struct KArgs {
+    const double *res;  // resistance (or conductance), ny x nx
+    const double *src;  // sources, ny x nx
+    int64_t nx, ny;
+    int R, D, W, bs, br, nbx, nby;
+    int ric, series, four, fp, correct;
+    // conditions
+    const double *cond_present[2];
+    const double *cond_future[2];
+    int cond_equal[2];
+    double cond_lo[2], cond_hi[2];
+    const double *cond_val;  // per target: 2 block values
+    // targets
+    const int *count_ptr;   // number of targets (device)
+    const int *targets;     // lattice ids of the targets, in lattice order
+    const double *lat_amps; // per lattice point: the block's source sum
+    const double *corr;     // W x W correction factors, or null
+    // outputs of a batch
+    double *cur_win;  // batch slots of W*W doubles (pitch w of each window)
+    double *fp_win;
+    WinStat *stat;    // per target: [land, flow]
+    int *queue;       // work counter of this launch
+    int batch_start, batch_size;
+    // working memory
+    char *gscratch;   // gridDim.x slices of lay.gmem_bytes
+    ArenaLayout lay;
+    SolveParams sp;
+    int mode;         // 0 windows of targets, 1 the two correction windows
+    double n_corr_sources;  // cells within radius of the correction disk (mode 1)
+    // adjoint (mode 2): weights of J on the map; per-window gradient slots
+    const double *weight;
+};
+
+template <typename X>
+__device__ __forceinline__ X *arena_ptr(const ArenaLayout &L, int a, char *sm, char *gm) {
+    const uint32_t o = L.off[a];
+    return reinterpret_cast<X *>((o & 0x80000000u) ? gm + (o & 0x7fffffffu) : sm + o);
+}
+
+// Scalar type traits for the inner solve.
+template <typename T>
+struct Sentinel;
+template <>
+struct Sentinel<float> {
+    __device__ static float neg() { return -CUDART_INF_F; }
+    __device__ static float pos() { return CUDART_INF_F; }
+};
+template <>
+struct Sentinel<double> {
+    __device__ static double neg() { return -CUDART_INF; }
+    __device__ static double pos() { return CUDART_INF; }
+};
+
+__device__ __forceinline__ float tmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double tmax(double a, double b) { return fmax(a, b); }
+
+// Block-wide ordered compaction of flags over [0, n): out[k] = i of the k-th
+// flagged i (increasing).  Returns the count.  scan: shared, >= 33 ints.
+template <int NT, typename F>
+__device__ int block_compact(int n, F flag, uint16_t *out, int *scan) {
+    constexpr int NW = NT / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int base = 0;
+    for (int c0 = 0; c0 < n; c0 += NT) {
+        const int i = c0 + threadIdx.x;
+        const bool f = i < n && flag(i);
+        const unsigned m = __ballot_sync(0xffffffffu, f);
+        if (lane == 0) scan[warp] = __popc(m);
+        __syncthreads();
+        int before = 0, total = 0;
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+            const int c = scan[k];
+            before += k < warp ? c : 0;
+            total += c;
+        }
+        if (f) out[base + before + __popc(m & ((1u << lane) - 1u))] = static_cast<uint16_t>(i);
+        base += total;
+        __syncthreads();
+    }
+    return base;
+}
+
+// ---------------------------------------------------------------------------
+// The solver of one window.
+// ---------------------------------------------------------------------------
+template <int NT, typename T, bool FOUR, bool MG, bool REFINE>
+struct Win {
+    using NB = Nb<FOUR>;
+    static constexpr int ND = NB::ND, LOWER = NB::LOWER;
+
+    const KArgs &a;
+    char *sm, *gm;
+    Reducer<NT> &red;
+    int *scan;       // shared scratch (>= 64 ints)
+    int *lvh, *lvw;  // shared: level dimensions
+    WinGeom G;
+    int nu = 0;      // number of unknowns
+    int nlev = 1;
+
+    __device__ Win(const KArgs &a_, char *sm_, char *gm_, Reducer<NT> &red_, int *scan_, int *lvh_, int *lvw_)
+        : a(a_), sm(sm_), gm(gm_), red(red_), scan(scan_), lvh(lvh_), lvw(lvw_) {}
+
+    template <typename X>
+    __device__ __forceinline__ X *A(int k) const { return arena_ptr<X>(a.lay, k, sm, gm); }
+    template <typename X>
+    __device__ __forceinline__ X *LV(int l, int k) const {
+        return arena_ptr<X>(a.lay, AR_LEVEL + (l - 1) * LV_COUNT + k, sm, gm);
+    }
+    __device__ __forceinline__ int noff(int d) const { return NB::dy(d) * G.P + NB::dx(d); }
+
+    // ---- 1. window data ----------------------------------------------------
+    // Conductance, candidates and raw sources (omniscape.cpp:495-519).  FLOW
+    // keeps the sources the LAND pass scaled.  Returns the sum of positive raw
+    // sources (the scaling denominator; 0 for FLOW).
+    __device__ double load(int kind, double amps) {
+        uint8_t *mask = A<uint8_t>(AR_MASK);
+        double *g64 = A<double>(AR_G64), *x64 = A<double>(AR_X64), *b64 = A<double>(AR_B64);
+        const int h = G.h, w = G.w, P = G.P, NP = G.NP;
+        const int R = a.R, D = a.D, br = a.br;
+        const int64_t ylim = (D + br < a.ny - 1 ? D + br : a.ny - 1), xlim = (D + br < a.nx - 1 ? D + br : a.nx - 1);
+        double pos = 0.0;
+        for (int i = threadIdx.x; i < NP; i += NT) {
+            const int py = i / P, y = py - 1, x = i - py * P - 1;
+            double g = 0.0, raw = 0.0;
+            uint8_t m = 0;
+            if (y >= 0 && y < h && x >= 0 && x < w) {
+                const int dy = y - G.gy, dx = x - G.gx, d2 = dy * dy + dx * dx;
+                if (kind == KIND_LAND) {
+                    const double r = a.res[(G.y0 + y) * a.nx + (G.x0 + x)];
+                    g = -9999.0;
+                    if (d2 <= D * D && !isnan(r)) g = a.ric ? r : 1.0 / r;
+                    if (d2 <= R * R) {
+                        raw = a.src[(G.y0 + y) * a.nx + (G.x0 + x)];
+                        if (isnan(raw)) raw = 0.0;
+                    }
+                } else if (kind == KIND_FLOW) {
+                    g = 1.0;
+                } else {
+                    g = d2 <= D * D ? 1.0 : -9999.0;
+                    raw = d2 <= R * R ? 1.0 : 0.0;
+                    if (kind == KIND_CORR_NULL && dy == 0 && dx == 0) raw = 0.0;
+                }
+                if (kind == KIND_LAND || kind == KIND_CORR_BLOCK) {
+                    // the target block zeroed at radius + buffer from the corner (omniscape.cpp:517-519)
+                    if (y >= D - br && y <= ylim && x >= D - br && x <= xlim) raw = 0.0;
+                }
+                if (g > 0) m = M_CAND;
+                if (kind != KIND_FLOW) {
+                    b64[i] = raw;
+                    if (raw > 0) pos += raw;
+                }
+            } else if (kind != KIND_FLOW) {
+                b64[i] = 0.0;
+            }
+            g64[i] = g;
+            mask[i] = m;
+            x64[i] = 0.0;
+        }
+        if (kind == KIND_FLOW) {
+            __syncthreads();
+            return 0.0;
+        }
+        const double sum = red.sum(pos);  // ends with a barrier
+        // rescale the positive sources to the block's amps (omniscape.cpp:520-525)
+        if (kind == KIND_CORR_NULL) {
+            const double v = 1.0 / (a.n_corr_sources - 1.0);
+            for (int i = threadIdx.x; i < NP; i += NT)
+                if (b64[i] != 0.0) b64[i] = v;
+        } else {
+            if (kind == KIND_CORR_BLOCK) amps = static_cast<double>(a.bs) * a.bs;
+            for (int i = threadIdx.x; i < NP; i += NT) {
+                const double v = b64[i];
+                if (v > 0) b64[i] = (v * amps) / sum;
+            }
+        }
+        __syncthreads();
+        return sum;
+    }
+
+    // Conditions (omniscape.cpp:526-530, match_condition :218-230).
+    __device__ void apply_conditions(double v1, double v2) {
+        double *b64 = A<double>(AR_B64);
+        for (int k = 0; k < 2; ++k) {
+            const double *c = a.cond_present[k];
+            if (!c) continue;
+            const double val = k == 0 ? v1 : v2;
+            for (int i = threadIdx.x; i < G.NP; i += NT) {
+                const int py = i / G.P, y = py - 1, x = i - py * G.P - 1;
+                if (y < 0 || y >= G.h || x < 0 || x >= G.w) continue;
+                const double v = c[(G.y0 + y) * a.nx + (G.x0 + x)];
+                if (isnan(v)) continue;
+                if (a.cond_equal[k]) {
+                    if (v != val) b64[i] = 0.0;
+                } else {
+                    const double dd = v - val;
+                    if (dd > a.cond_hi[k] || dd < a.cond_lo[k]) b64[i] = 0.0;
+                }
+            }
+            __syncthreads();
+        }
+    }
+
+    // ---- 2. the ground's component -----------------------------------------
+    // Monotone label propagation until no cell changes; bounded by the number
+    // of cells (every productive sweep adds one).  Returns false when the
+    // ground has no node.
+    __device__ bool flood(int kind) {
+        uint8_t *mask = A<uint8_t>(AR_MASK);
+        const int ground = (G.gy + 1) * G.P + G.gx + 1;
+        if (kind == KIND_FLOW) {
+            for (int i = threadIdx.x; i < G.NP; i += NT)
+                if (mask[i] & M_CAND) mask[i] = M_CAND | M_PRESENT;
+            __syncthreads();
+            return true;
+        }
+        const bool has = mask[ground] & M_CAND;
+        __syncthreads();
+        if (!has) return false;
+        if (threadIdx.x == 0) mask[ground] = M_CAND | M_PRESENT;
+        __syncthreads();
+        int sweep = 0;
+        while (true) {
+            int changed = 0;
+            const bool fwd = (sweep & 1) == 0;
+            const int start = fwd ? static_cast<int>(threadIdx.x) : G.NP - 1 - static_cast<int>(threadIdx.x);
+            for (int i = start; fwd ? i < G.NP : i >= 0; i += fwd ? NT : -NT) {
+                const uint8_t m = mask[i];
+                if ((m & (M_CAND | M_PRESENT)) != M_CAND) continue;
+                bool any = false;
+#pragma unroll
+                for (int d = 0; d < ND; ++d) any |= (static_cast<volatile uint8_t *>(mask)[i + noff(d)] & M_PRESENT) != 0;
+                if (any) {
+                    mask[i] = m | M_PRESENT;
+                    changed = 1;
+                }
+            }
+            ++sweep;
+            if (!__syncthreads_or(changed)) break;
+        }
+        return true;
+    }
+
+    // Sum of the sources over the unknowns-to-be (omniscape.cpp:101, 149-150);
+    // marks the unknowns and lists them.
+    __device__ double mark_unknowns() {
+        uint8_t *mask = A<uint8_t>(AR_MASK);
+        const double *b64 = A<double>(AR_B64);
+        const int ground = (G.gy + 1) * G.P + G.gx + 1;
+        double t = 0.0;
+        for (int i = threadIdx.x; i < G.NP; i += NT) {
+            uint8_t m = mask[i];
+            if ((m & M_PRESENT) && i != ground) {
+                m |= M_UNKNOWN;
+                t += b64[i];
+            }
+            mask[i] = m;
+        }
+        const double total = red.sum(t);
+        nu = block_compact<NT>(G.NP, [&](int i) { return (mask[i] & M_UNKNOWN) != 0; }, A<uint16_t>(AR_ULIST), scan);
+        return total;
+    }
+
+    // ---- 3. assembly -------------------------------------------------------
+    // Diagonal summed in column-major neighbour order with the 10 eps shift
+    // (system.cpp:458-487); stencil conductances with sentinels off the nodes.
+    __device__ void assemble() {
+        const uint8_t *mask = A<uint8_t>(AR_MASK);
+        const double *g64 = A<double>(AR_G64);
+        T *gT = A<T>(AR_GT), *invd = A<T>(AR_INVD), *z = A<T>(AR_Z);
+        T *d = A<T>(AR_D), *r = A<T>(AR_R), *p = A<T>(AR_P), *q = A<T>(AR_Q);
+        const bool series = a.series;
+        for (int i = threadIdx.x; i < G.NP; i += NT) {
+            const uint8_t m = mask[i];
+            const double g = g64[i];
+            gT[i] = (m & M_PRESENT) ? static_cast<T>(series ? 1.0 / g : g)
+                                    : (series ? Sentinel<T>::pos() : Sentinel<T>::neg());
+            invd[i] = T(0);
+            p[i] = T(0);
+            q[i] = T(0);
+            r[i] = T(0);
+            if (!(REFINE == false && sizeof(T) == 8)) d[i] = T(0);
+            if (MG) z[i] = T(0);
+        }
+        __syncthreads();
+        const uint16_t *ul = A<uint16_t>(AR_ULIST);
+        for (int k = threadIdx.x; k < nu; k += NT) {
+            const int i = ul[k];
+            const double gi = g64[i];
+            double diag = 0.0;
+#pragma unroll
+            for (int dd = 0; dd < ND; ++dd) {
+                const int n = i + noff(dd);
+                if (mask[n] & M_PRESENT) diag += edge_w_exact(gi, g64[n], NB::diag(dd), series);
+            }
+            invd[i] = static_cast<T>(1.0 / (diag + kShift));
+            if (MG) z[i] = static_cast<T>(diag);
+        }
+        __syncthreads();
+    }
+
+    // ---- level-0 operator in T ---------------------------------------------
+    // (A x)_i = sum_d w_id (x_i - x_n); w from the stencil conductances
+    // (sentinels give w = 0 off the nodes; x = 0 off the unknowns).
+    __device__ __forceinline__ T apply0(const T *gT, const T *x, int i) const {
+        const T gi = gT[i], xi = x[i];
+        T ao = T(0), ad = T(0);
+        if (a.series) {
+#pragma unroll
+            for (int dd = 0; dd < ND; ++dd) {
+                const int n = i + noff(dd);
+                const T wv = T(2) / (gi + gT[n]);
+                if (NB::diag(dd))
+                    ad += wv * (xi - x[n]);
+                else
+                    ao += wv * (xi - x[n]);
+            }
+            return ao + ad * T(0.70710678118654752440);
+        }
+#pragma unroll
+        for (int dd = 0; dd < ND; ++dd) {
+            const int n = i + noff(dd);
+            const T wv = tmax(gi + gT[n], T(0));
+            if (NB::diag(dd))
+                ad += wv * (xi - x[n]);
+            else
+                ao += wv * (xi - x[n]);
+        }
+        return ao * T(0.5) + ad * T(kInvTwoSqrt2);
+    }
+
+    // A level-0 entry A(i, i+s) for RAP (s = (sy, sx) in {-1,0,1}^2).
+    __device__ __forceinline__ T entry0(int i, int sy, int sx) const {
+        const uint8_t *mask = A<uint8_t>(AR_MASK);
+        if (sy == 0 && sx == 0) return A<T>(AR_Z)[i];
+        if (FOUR && sy != 0 && sx != 0) return T(0);
+        const int n = i + sy * G.P + sx;
+        if (!(mask[n] & M_UNKNOWN)) return T(0);
+        const T *gT = A<T>(AR_GT);
+        const bool dg = sy != 0 && sx != 0;
+        if (a.series) {
+            const T wv = T(2) / (gT[i] + gT[n]);
+            return -(dg ? wv * T(0.70710678118654752440) : wv);
+        }
+        const T wv = tmax(gT[i] + gT[n], T(0));
+        return -(dg ? wv * T(kInvTwoSqrt2) : wv * T(0.5));
+    }
+
+    // A coarse entry A_l(i, i+s) from the symmetric storage.
+    __device__ __forceinline__ T entryc(int l, int i, int sy, int sx) const {
+        const int P = lvw[l] + 2;
+        if (sy == 0 && sx == 0) return LV<T>(l, LV_C0)[i];
+        if (sy == 0 && sx == 1) return LV<T>(l, LV_CE)[i];
+        if (sy == 1 && sx == -1) return LV<T>(l, LV_CSW)[i];
+        if (sy == 1 && sx == 0) return LV<T>(l, LV_CS)[i];
+        if (sy == 1 && sx == 1) return LV<T>(l, LV_CSE)[i];
+        if (sy == 0 && sx == -1) return LV<T>(l, LV_CE)[i - 1];
+        if (sy == -1 && sx == 1) return LV<T>(l, LV_CSW)[i - P + 1];
+        if (sy == -1 && sx == 0) return LV<T>(l, LV_CS)[i - P];
+        return LV<T>(l, LV_CSE)[i - P - 1];  // (-1, -1)
+    }
+    __device__ __forceinline__ T applyc(int l, const T *x, int i) const {
+        const int P = lvw[l] + 2;
+        const T *c0 = LV<T>(l, LV_C0), *cE = LV<T>(l, LV_CE), *cSW = LV<T>(l, LV_CSW), *cS = LV<T>(l, LV_CS),
+                *cSE = LV<T>(l, LV_CSE);
+        T s = c0[i] * x[i];
+        s += cE[i] * x[i + 1] + cSW[i] * x[i + P - 1] + cS[i] * x[i + P] + cSE[i] * x[i + P + 1];
+        s += cE[i - 1] * x[i - 1] + cSW[i - P + 1] * x[i - P + 1] + cS[i - P] * x[i - P] + cSE[i - P - 1] * x[i - P - 1];
+        return s;
+    }
+    __device__ __forceinline__ bool active(int l, int i) const {
+        if (l == 0) return (A<uint8_t>(AR_MASK)[i] & M_UNKNOWN) != 0;
+        return LV<T>(l, LV_INVD)[i] != T(0);
+    }
+
+    // ---- multigrid set-up (Galerkin R A P, masked bilinear P) -------------
+    __device__ void mg_setup() {
+        nlev = mg_levels(G.h, G.w);
+        if (threadIdx.x == 0) {
+            int h = G.h, w = G.w;
+            for (int l = 0; l < nlev; ++l) {
+                lvh[l] = h;
+                lvw[l] = w;
+                h = coarse_dim(h);
+                w = coarse_dim(w);
+            }
+        }
+        __syncthreads();
+        for (int l = 1; l < nlev; ++l) {
+            const int hf = lvh[l - 1], wf = lvw[l - 1], Pf = wf + 2;
+            const int hc = lvh[l], wc = lvw[l], Pc = wc + 2, NPc = (hc + 2) * Pc;
+            const bool cy = hc != hf, cx = wc != wf;
+            T *c0 = LV<T>(l, LV_C0), *cE = LV<T>(l, LV_CE), *cSW = LV<T>(l, LV_CSW), *cS = LV<T>(l, LV_CS),
+              *cSE = LV<T>(l, LV_CSE), *iv = LV<T>(l, LV_INVD), *x = LV<T>(l, LV_X), *b = LV<T>(l, LV_B),
+              *t = LV<T>(l, LV_T);
+            for (int J = threadIdx.x; J < NPc; J += NT) {
+                const int jpy = J / Pc, jy = jpy - 1, jx = J - jpy * Pc - 1;
+                T acc[5] = {T(0), T(0), T(0), T(0), T(0)};
+                bool act = false;
+                if (jy >= 0 && jy < hc && jx >= 0 && jx < wc) {
+                    for (int ay = (cy ? -1 : 0); ay <= (cy ? 1 : 0); ++ay) {
+                        const int fy = cy ? 2 * jy + ay : jy;
+                        if (fy < 0 || fy >= hf) continue;
+                        const T wa = ay == 0 ? T(1) : T(0.5);
+                        for (int ax = (cx ? -1 : 0); ax <= (cx ? 1 : 0); ++ax) {
+                            const int fx = cx ? 2 * jx + ax : jx;
+                            if (fx < 0 || fx >= wf) continue;
+                            const int i = (fy + 1) * Pf + fx + 1;
+                            if (!active(l - 1, i)) continue;
+                            act = true;
+                            const T wi = wa * (ax == 0 ? T(1) : T(0.5));
+                            for (int sy = -1; sy <= 1; ++sy)
+                                for (int sx = -1; sx <= 1; ++sx) {
+                                    const T aij = l == 1 ? entry0(i, sy, sx) : entryc(l - 1, i, sy, sx);
+                                    if (aij == T(0)) continue;
+                                    const int gy = fy + sy, gx = fx + sx;  // fine j
+                                    const T base = wi * aij;
+                                    // coarse K = J + e, e in {C, E, SW, S, SE}
+#pragma unroll
+                                    for (int e = 0; e < 5; ++e) {
+                                        const int ey = e == 0 ? 0 : e == 1 ? 0 : 1;
+                                        const int ex = e == 0 ? 0 : e == 1 ? 1 : e == 2 ? -1 : e == 3 ? 0 : 1;
+                                        const int ky = jy + ey, kx = jx + ex;
+                                        if (ky >= hc || kx < 0 || kx >= wc) continue;
+                                        T py, px;
+                                        if (cy) {
+                                            const int dd = gy - 2 * ky;
+                                            py = dd == 0 ? T(1) : (dd == 1 || dd == -1) ? T(0.5) : T(0);
+                                        } else {
+                                            py = gy == ky ? T(1) : T(0);
+                                        }
+                                        if (cx) {
+                                            const int dd = gx - 2 * kx;
+                                            px = dd == 0 ? T(1) : (dd == 1 || dd == -1) ? T(0.5) : T(0);
+                                        } else {
+                                            px = gx == kx ? T(1) : T(0);
+                                        }
+                                        acc[e] += base * py * px;
+                                    }
+                                }
+                        }
+                    }
+                }
+                c0[J] = act ? acc[0] : T(0);
+                cE[J] = act ? acc[1] : T(0);
+                cSW[J] = act ? acc[2] : T(0);
+                cS[J] = act ? acc[3] : T(0);
+                cSE[J] = act ? acc[4] : T(0);
+                iv[J] = act ? static_cast<T>(a.sp.omega) / acc[0] : T(0);
+                x[J] = T(0);
+                b[J] = T(0);
+                t[J] = T(0);
+            }
+            __syncthreads();
+            // entries towards inactive cells were accumulated through P rows of
+            // inactive fine cells only, which are zero: nothing to clear.
+        }
+        dense_setup();
+    }
+
+    // Pseudo-inverse of the coarsest operator (at most kNcMax cells): Cholesky
+    // with skipped (near-zero) pivots, then one column of the inverse per lane.
+    __device__ void dense_setup() {
+        double *M = A<double>(AR_DENSE);
+        const int l = nlev - 1;
+        const int hc = lvh[l], wc = lvw[l], Pc = wc + 2, n = hc * wc;
+        for (int e = threadIdx.x; e < kNcMax * kNcMax; e += NT) {
+            const int u = e / kNcMax, v = e - u * kNcMax;
+            double val = 0.0;
+            if (u < n && v < n) {
+                const int uy = u / wc, ux = u - uy * wc, vy = v / wc, vx = v - vy * wc;
+                const int sy = vy - uy, sx = vx - ux;
+                const int iu = (uy + 1) * Pc + ux + 1;
+                if (sy >= -1 && sy <= 1 && sx >= -1 && sx <= 1) {
+                    if (!active(l, iu) || !active(l, (vy + 1) * Pc + vx + 1))
+                        val = (u == v) ? 1.0 : 0.0;
+                    else
+                        val = static_cast<double>(l == 0 ? entry0(iu, sy, sx) : entryc(l, iu, sy, sx));
+                }
+            }
+            M[e] = val;
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            const int lane = threadIdx.x;
+            // in-place lower Cholesky; skipped pivots get L = identity column
+            __shared__ unsigned skip_bits;
+            if (lane == 0) skip_bits = 0u;
+            __syncwarp();
+            const double od = lane < n ? M[lane * kNcMax + lane] : 0.0;  // original diagonal
+            for (int k = 0; k < n; ++k) {
+                const double piv = M[k * kNcMax + k];
+                const double odk = __shfl_sync(0xffffffffu, od, k);
+                // a Schur-complement pivot that vanished against the original diagonal: a
+                // dependent direction of the masked prolongation; left out of the inverse
+                const bool skip = !(piv > 1e-10 * odk);
+                if (skip) {
+                    if (lane == 0) skip_bits |= 1u << k;
+                    if (lane < n) {
+                        M[lane * kNcMax + k] = lane == k ? 1.0 : 0.0;
+                    }
+                    __syncwarp();
+                    continue;
+                }
+                const double lkk = sqrt(piv);
+                __syncwarp();
+                if (lane > k && lane < n) M[lane * kNcMax + k] /= lkk;
+                if (lane == k) M[k * kNcMax + k] = lkk;
+                __syncwarp();
+                if (lane > k && lane < n) {
+                    const double lik = M[lane * kNcMax + k];
+                    for (int j = k + 1; j <= lane; ++j) M[lane * kNcMax + j] -= lik * M[j * kNcMax + k];
+                }
+                __syncwarp();
+            }
+            const unsigned sk = skip_bits;
+            // column c of the inverse, in the strictly upper triangle + a copy:
+            // solve L y = e_c, then L^T x = y, skipping skipped unknowns.
+            double col[kNcMax];
+            if (lane < n) {
+                for (int i = 0; i < n; ++i) col[i] = 0.0;
+                if (!((sk >> lane) & 1u)) col[lane] = 1.0;
+                for (int i = 0; i < n; ++i) {
+                    if ((sk >> i) & 1u) {
+                        col[i] = 0.0;
+                        continue;
+                    }
+                    double s = col[i];
+                    for (int k = 0; k < i; ++k) s -= M[i * kNcMax + k] * col[k];
+                    col[i] = s / M[i * kNcMax + i];
+                }
+                for (int i = n - 1; i >= 0; --i) {
+                    if ((sk >> i) & 1u) {
+                        col[i] = 0.0;
+                        continue;
+                    }
+                    double s = col[i];
+                    for (int k = i + 1; k < n; ++k) s -= M[k * kNcMax + i] * col[k];
+                    col[i] = s / M[i * kNcMax + i];
+                }
+            }
+            __syncwarp();
+            // store the inverse in the upper triangle rows (i <= c): M[c][i] for i >= c is free? use
+            // the transposed store into the strictly upper part plus the diagonal, after all reads.
+            if (lane < n)
+                for (int i = 0; i < n; ++i)
+                    if (i >= lane) M[lane * kNcMax + i] = col[i];  // row lane, columns >= lane (symmetric)
+        }
+        __syncthreads();
+    }
+
+    // z = B r: one V(1,1) cycle, damped-Jacobi smoothing, exact coarsest.
+    // r is level-0 (unknowns only); the result goes to AR_Q; AR_Z is scratch.
+    __device__ void vcycle(const T *r) {
+        const uint16_t *ul = A<uint16_t>(AR_ULIST);
+        const T *gT = A<T>(AR_GT), *invd = A<T>(AR_INVD);
+        T *z = A<T>(AR_Z), *q = A<T>(AR_Q);
+        const T om = static_cast<T>(a.sp.omega);
+        for (int k = threadIdx.x; k < nu; k += NT) {
+            const int i = ul[k];
+            z[i] = om * invd[i] * r[i];
+        }
+        __syncthreads();
+        if (nlev == 1) {
+            // the window is its own coarsest level
+            coarse_solve(0, r, z);
+            __syncthreads();
+            for (int k = threadIdx.x; k < nu; k += NT) {
+                const int i = ul[k];
+                q[i] = z[i];
+            }
+            __syncthreads();
+            return;
+        }
+        for (int k = threadIdx.x; k < nu; k += NT) {
+            const int i = ul[k];
+            q[i] = r[i] - apply0(gT, z, i);
+        }
+        __syncthreads();
+        restrict_to(1, q);
+        for (int l = 1; l < nlev - 1; ++l) {
+            const int NPc = (lvh[l] + 2) * (lvw[l] + 2);
+            T *x = LV<T>(l, LV_X), *b = LV<T>(l, LV_B), *t = LV<T>(l, LV_T);
+            const T *iv = LV<T>(l, LV_INVD);
+            for (int i = threadIdx.x; i < NPc; i += NT) x[i] = iv[i] * b[i];
+            __syncthreads();
+            for (int i = threadIdx.x; i < NPc; i += NT)
+                if (iv[i] != T(0)) t[i] = b[i] - applyc(l, x, i);
+            __syncthreads();
+            restrict_to(l + 1, t);
+        }
+        coarse_solve(nlev - 1, LV<T>(nlev - 1, LV_B), LV<T>(nlev - 1, LV_X));
+        __syncthreads();
+        for (int l = nlev - 2; l >= 1; --l) {
+            const int NPc = (lvh[l] + 2) * (lvw[l] + 2);
+            T *x = LV<T>(l, LV_X), *b = LV<T>(l, LV_B), *t = LV<T>(l, LV_T);
+            const T *iv = LV<T>(l, LV_INVD);
+            const T *xc = LV<T>(l + 1, l + 1 == nlev - 1 ? LV_X : LV_T);
+            prolong_add(l, x, xc);
+            __syncthreads();
+            for (int i = threadIdx.x; i < NPc; i += NT)
+                if (iv[i] != T(0)) t[i] = x[i] + iv[i] * (b[i] - applyc(l, x, i));
+            __syncthreads();
+        }
+        prolong_add(0, z, LV<T>(1, nlev - 1 == 1 ? LV_X : LV_T));
+        __syncthreads();
+        for (int k = threadIdx.x; k < nu; k += NT) {
+            const int i = ul[k];
+            q[i] = z[i] + om * invd[i] * (r[i] - apply0(gT, z, i));
+        }
+        __syncthreads();
+    }
+
+    // b_{l} = P^T t_{l-1} (level l-1 residual, zero off its active cells).
+    __device__ void restrict_to(int l, const T *tf) {
+        const int hf = lvh[l - 1], wf = lvw[l - 1], Pf = wf + 2;
+        const int hc = lvh[l], wc = lvw[l], Pc = wc + 2, NPc = (hc + 2) * Pc;
+        const bool cy = hc != hf, cx = wc != wf;
+        T *b = LV<T>(l, LV_B);
+        const T *iv = LV<T>(l, LV_INVD);
+        for (int J = threadIdx.x; J < NPc; J += NT) {
+            if (iv[J] == T(0)) continue;
+            const int jpy = J / Pc, jy = jpy - 1, jx = J - jpy * Pc - 1;
+            T s = T(0);
+            for (int ay = (cy ? -1 : 0); ay <= (cy ? 1 : 0); ++ay) {
+                const int fy = cy ? 2 * jy + ay : jy;
+                if (fy < 0 || fy >= hf) continue;
+                const T wa = ay == 0 ? T(1) : T(0.5);
+                for (int ax = (cx ? -1 : 0); ax <= (cx ? 1 : 0); ++ax) {
+                    const int fx = cx ? 2 * jx + ax : jx;
+                    if (fx < 0 || fx >= wf) continue;
+                    s += wa * (ax == 0 ? T(1) : T(0.5)) * tf[(fy + 1) * Pf + fx + 1];
+                }
+            }
+            b[J] = s;
+        }
+        __syncthreads();
+    }
+
+    // x_l += P x_{l+1} on the active cells of level l.
+    __device__ void prolong_add(int l, T *x, const T *xc) {
+        const int hf = lvh[l], wf = lvw[l], Pf = wf + 2, NPf = (hf + 2) * Pf;
+        const int hc = lvh[l + 1], wc = lvw[l + 1], Pc = wc + 2;
+        const bool cy = hc != hf, cx = wc != wf;
+        auto one = [&](int i) {
+            const int py = i / Pf, fy = py - 1, fx = i - py * Pf - 1;
+            int y0, y1, x0, x1;
+            T wy0, wy1, wx0, wx1;
+            if (cy) {
+                y0 = fy >> 1;
+                y1 = (fy & 1) ? y0 + 1 : y0;
+                wy0 = (fy & 1) ? T(0.5) : T(1);
+                wy1 = (fy & 1) ? T(0.5) : T(0);
+            } else {
+                y0 = y1 = fy;
+                wy0 = T(1);
+                wy1 = T(0);
+            }
+            if (cx) {
+                x0 = fx >> 1;
+                x1 = (fx & 1) ? x0 + 1 : x0;
+                wx0 = (fx & 1) ? T(0.5) : T(1);
+                wx1 = (fx & 1) ? T(0.5) : T(0);
+            } else {
+                x0 = x1 = fx;
+                wx0 = T(1);
+                wx1 = T(0);
+            }
+            const T v = wy0 * (wx0 * xc[(y0 + 1) * Pc + x0 + 1] + wx1 * xc[(y0 + 1) * Pc + x1 + 1]) +
+                        wy1 * (wx0 * xc[(y1 + 1) * Pc + x0 + 1] + wx1 * xc[(y1 + 1) * Pc + x1 + 1]);
+            x[i] += v;
+        };
+        if (l == 0) {
+            const uint16_t *ul = A<uint16_t>(AR_ULIST);
+            for (int k = threadIdx.x; k < nu; k += NT) one(ul[k]);
+        } else {
+            const T *iv = LV<T>(l, LV_INVD);
+            for (int i = threadIdx.x; i < NPf; i += NT)
+                if (iv[i] != T(0)) one(i);
+        }
+    }
+
+    // x = M^+ b on the coarsest level l (its cells in row-major order).
+    __device__ void coarse_solve(int l, const T *b, T *x) {
+        const double *M = A<double>(AR_DENSE);
+        const int hc = lvh[l], wc = lvw[l], Pc = wc + 2, n = hc * wc;
+        if (threadIdx.x < n) {
+            const int u = threadIdx.x;
+            double s = 0.0;
+            for (int v = 0; v < n; ++v) {
+                const double m = v >= u ? M[u * kNcMax + v] : M[v * kNcMax + u];
+                s += m * static_cast<double>(b[(v / wc + 1) * Pc + v % wc + 1]);
+            }
+            const int iu = (u / wc + 1) * Pc + u % wc + 1;
+            if (l == 0) {
+                if (A<uint8_t>(AR_MASK)[iu] & M_UNKNOWN) x[iu] = static_cast<T>(s);
+            } else {
+                x[iu] = static_cast<T>(s);
+            }
+        }
+    }
+
+    // ---- preconditioned CG on the T operator -------------------------------
+    // Solves A d = r0 (r holds r0 on entry, the residual on exit) to relative
+    // residual rtol or for at most maxit iterations.  d must be 0 on entry.
+    // Returns the iterations; *ok = false on breakdown.
+    __device__ int pcg(T *d, T *r, double rtol, int maxit, bool use_mg, bool *ok) {
+        const uint16_t *ul = A<uint16_t>(AR_ULIST);
+        const T *gT = A<T>(AR_GT), *invd = A<T>(AR_INVD);
+        T *p = A<T>(AR_P), *q = A<T>(AR_Q);
+        *ok = true;
+        double rz = 0.0, rr = 0.0;
+        if (MG && use_mg) {
+            vcycle(r);
+            for (int k = threadIdx.x; k < nu; k += NT) {
+                const int i = ul[k];
+                const T zi = q[i];
+                p[i] = zi;
+                rz += static_cast<double>(r[i]) * static_cast<double>(zi);
+                rr += static_cast<double>(r[i]) * static_cast<double>(r[i]);
+            }
+        } else {
+            for (int k = threadIdx.x; k < nu; k += NT) {
+                const int i = ul[k];
+                const T zi = invd[i] * r[i];
+                p[i] = zi;
+                rz += static_cast<double>(r[i]) * static_cast<double>(zi);
+                rr += static_cast<double>(r[i]) * static_cast<double>(r[i]);
+            }
+        }
+        red.sum2(rz, rr);  // barrier: p visible
+        const double stop = rtol * rtol * rr;
+        if (rr == 0.0) return 0;
+        int it = 0;
+        while (it < maxit) {
+            double pq = 0.0;
+            for (int k = threadIdx.x; k < nu; k += NT) {
+                const int i = ul[k];
+                const T qi = apply0(gT, p, i);
+                q[i] = qi;
+                pq += static_cast<double>(p[i]) * static_cast<double>(qi);
+            }
+            pq = red.sum(pq);
+            ++it;
+            if (!(pq > 0.0) || !isfinite(pq)) {
+                *ok = false;
+                break;
+            }
+            const T alpha = static_cast<T>(rz / pq);
+            double rz2 = 0.0, rr2 = 0.0;
+            if (MG && use_mg) {
+                for (int k = threadIdx.x; k < nu; k += NT) {
+                    const int i = ul[k];
+                    d[i] += alpha * p[i];
+                    r[i] -= alpha * q[i];
+                }
+                __syncthreads();
+                vcycle(r);
+                for (int k = threadIdx.x; k < nu; k += NT) {
+                    const int i = ul[k];
+                    rz2 += static_cast<double>(r[i]) * static_cast<double>(q[i]);
+                    rr2 += static_cast<double>(r[i]) * static_cast<double>(r[i]);
+                }
+            } else {
+                for (int k = threadIdx.x; k < nu; k += NT) {
+                    const int i = ul[k];
+                    d[i] += alpha * p[i];
+                    const T ri = r[i] - alpha * q[i];
+                    r[i] = ri;
+                    rz2 += static_cast<double>(ri) * static_cast<double>(invd[i] * ri);
+                    rr2 += static_cast<double>(ri) * static_cast<double>(ri);
+                }
+            }
+            red.sum2(rz2, rr2);
+            if (!isfinite(rr2)) {
+                *ok = false;
+                break;
+            }
+            if (rr2 <= stop) break;
+            const T beta = static_cast<T>(rz2 / rz);
+            rz = rz2;
+            if (MG && use_mg) {
+                for (int k = threadIdx.x; k < nu; k += NT) {
+                    const int i = ul[k];
+                    p[i] = q[i] + beta * p[i];
+                }
+            } else {
+                for (int k = threadIdx.x; k < nu; k += NT) {
+                    const int i = ul[k];
+                    p[i] = invd[i] * r[i] + beta * p[i];
+                }
+            }
+            __syncthreads();
+        }
+        return it;
+    }
+
+    // r = b - A x in FP64 over the unknowns (exact weights up to the
+    // reciprocal of 2 sqrt 2), stored as T in AR_R; returns (||r||^2, ||b||^2).
+    __device__ void residual64(double *rr_out, double *bb_out, bool first) {
+        const uint8_t *mask = A<uint8_t>(AR_MASK);
+        const uint16_t *ul = A<uint16_t>(AR_ULIST);
+        const double *g64 = A<double>(AR_G64), *x64 = A<double>(AR_X64), *b64 = A<double>(AR_B64);
+        T *r = A<T>(AR_R);
+        const bool series = a.series;
+        double rr = 0.0, bb = 0.0;
+        for (int k = threadIdx.x; k < nu; k += NT) {
+            const int i = ul[k];
+            const double bi = b64[i];
+            double ri = bi;
+            if (!first) {
+                const double gi = g64[i], xi = x64[i];
+                double ao = 0.0, ad = 0.0;
+#pragma unroll
+                for (int dd = 0; dd < ND; ++dd) {
+                    const int n = i + noff(dd);
+                    if (!(mask[n] & M_PRESENT)) continue;
+                    const double gn = g64[n];
+                    const double wv = series ? 2.0 / (1.0 / gi + 1.0 / gn) : gi + gn;
+                    if (NB::diag(dd))
+                        ad += wv * (xi - x64[n]);
+                    else
+                        ao += wv * (xi - x64[n]);
+                }
+                const double ax = series ? ao + ad * (1.0 / kSqrt2) : ao * 0.5 + ad * kInvTwoSqrt2;
+                ri = bi - (ax + kShift * xi);
+            }
+            r[i] = static_cast<T>(ri);
+            rr += ri * ri;
+            bb += bi * bi;
+        }
+        red.sum2(rr, bb);
+        *rr_out = rr;
+        *bb_out = bb;
+    }
+
+    // ---- the solve ----------------------------------------------------------
+    __device__ void solve(WinStat *st) {
+        const uint16_t *ul = A<uint16_t>(AR_ULIST);
+        double *x64 = A<double>(AR_X64);
+        const bool want_mg = MG && a.sp.pc == 2;
+        if (MG && want_mg) mg_setup();
+        int iters = 0, outer = 0, status = 1;
+        double rel = 0.0;
+        if (!REFINE) {
+            // one CG run on the T = double operator, straight to the tolerance
+            T *d = sizeof(T) == 8 ? reinterpret_cast<T *>(x64) : A<T>(AR_D);
+            T *r = A<T>(AR_R);
+            double rr, bb;
+            residual64(&rr, &bb, true);  // r = b (barrier)
+            bool ok = true;
+            iters = pcg(d, r, a.sp.tol, a.sp.max_iter, want_mg, &ok);
+            outer = 1;
+            __syncthreads();
+            if (sizeof(T) != 8) {
+                for (int k = threadIdx.x; k < nu; k += NT) x64[ul[k]] = static_cast<double>(d[ul[k]]);
+                __syncthreads();
+            }
+            double rr2, bb2;
+            residual64(&rr2, &bb2, false);
+            rel = bb2 > 0 ? sqrt(rr2 / bb2) : 0.0;
+            if (!ok || !isfinite(rel)) status = 3;
+            else if (iters >= a.sp.max_iter && rel > a.sp.tol) status = 2;
+        } else {
+            T *d = A<T>(AR_D), *r = A<T>(AR_R);
+            bool use_mg = want_mg;
+            double prev = CUDART_INF;
+            int stalls = 0;
+            while (true) {
+                double rr, bb;
+                residual64(&rr, &bb, outer == 0);
+                rel = bb > 0 ? sqrt(rr / bb) : 0.0;
+                if (!isfinite(rel)) {
+                    status = 3;
+                    break;
+                }
+                if (rel <= a.sp.tol) break;
+                if (outer >= a.sp.max_outer || iters >= a.sp.max_iter) {
+                    status = 2;
+                    break;
+                }
+                if (rel > 0.5 * prev) {
+                    // the preconditioned inner solve stopped helping: fall back to Jacobi
+                    if (++stalls >= 2 && use_mg) use_mg = false;
+                }
+                prev = rel;
+                // scale the residual to unit norm for the inner solve
+                const double s = sqrt(rr);
+                const T inv = static_cast<T>(1.0 / s);
+                for (int k = threadIdx.x; k < nu; k += NT) {
+                    const int i = ul[k];
+                    r[i] *= inv;
+                    d[i] = T(0);
+                }
+                __syncthreads();
+                bool ok = true;
+                const int budget = a.sp.max_iter - iters;
+                const int it = pcg(d, r, a.sp.inner_tol, budget < 1 ? 1 : budget, use_mg, &ok);
+                iters += it;
+                ++outer;
+                for (int k = threadIdx.x; k < nu; k += NT) {
+                    const int i = ul[k];
+                    x64[i] += s * static_cast<double>(d[i]);
+                }
+                __syncthreads();
+                if (!ok && use_mg) use_mg = false;
+            }
+        }
+        if (threadIdx.x == 0 && st) {
+            st->iters = iters;
+            st->outer = outer;
+            st->status = status;
+            st->resid = static_cast<float>(rel);
+        }
+    }
+
+    // ---- 5. node currents (grid.cpp:19-71), correction, output --------------
+    // out: h x w doubles (pitch w); corr: W x W factors or null, (cy0, cx0) its
+    // slice origin.
+    __device__ void currents(double *out, const double *corr, int cy0, int cx0) {
+        const uint8_t *mask = A<uint8_t>(AR_MASK);
+        const double *g64 = A<double>(AR_G64), *v = A<double>(AR_X64);
+        const bool series = a.series;
+        double maxout = -CUDART_INF, maxin = -CUDART_INF;
+        for (int i = threadIdx.x; i < G.NP; i += NT) {
+            if (!(mask[i] & M_PRESENT)) continue;
+            const double gi = g64[i], vi = v[i];
+#pragma unroll
+            for (int dd = LOWER; dd < ND; ++dd) {
+                const int n = i + noff(dd);
+                if (!(mask[n] & M_PRESENT)) continue;
+                const double b = edge_w_exact(gi, g64[n], NB::diag(dd), series) * (v[n] - vi);
+                if (b > maxout) maxout = b;
+                if (-b > maxin) maxin = -b;
+            }
+        }
+        red.max2(maxout, maxin);
+        const int W = a.W;
+        for (int i = threadIdx.x; i < G.NP; i += NT) {
+            const int py = i / G.P, y = py - 1, x = i - py * G.P - 1;
+            if (y < 0 || y >= G.h || x < 0 || x >= G.w) continue;
+            double c = 0.0;
+            if (mask[i] & M_PRESENT) {
+                const double gi = g64[i], vi = v[i];
+                double inflow = 0.0, outflow = 0.0;
+#pragma unroll
+                for (int dd = 0; dd < ND; ++dd) {
+                    const int n = i + noff(dd);
+                    if (!(mask[n] & M_PRESENT)) continue;
+                    const double b = edge_w_exact(gi, g64[n], NB::diag(dd), series) * (v[n] - vi);
+                    if (b > 0) {
+                        if (!(fabs(b / maxin) < 1e-8)) inflow += b;
+                    } else if (b < 0) {
+                        if (!(fabs(b / maxout) < 1e-8)) outflow -= b;
+                    }
+                }
+                c = inflow > outflow ? inflow : outflow;
+                if (corr) c *= corr[(cy0 + y) * W + (cx0 + x)];
+            }
+            out[y * G.w + x] = c;
+        }
+        __syncthreads();
+    }
+};
+
+}  // namespace lsb
