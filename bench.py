@@ -1,0 +1,354 @@
+"""Benchmark of the Omniscape moving-window solve on B200 (one JSON line on rank 0).
+
+Workload (``omni_1024``): 1024 x 1024 Gaussian-random-field resistance 10^(2g) with ~1% NoData in 3 x 3
+clusters, source 1 where g < 0.3; radius 32, block 3, 8 neighbours, average-conductance edges; cumulative
+current.  A step is one full Omniscape run over the raster (every target window solved and scattered).
+
+* ``value``: windows/s of the FP32-CG + FP64-refinement solve with the rasters resident in HBM, device time
+  (CUDA events), L2 flushed between steps, max over ranks; every rank solves its own seeded raster (weak
+  scaling, no collective on the data path).
+* ``e2e``: the same metric through the drop-in ``landschaft_b200.omniscape(numpy, ...)`` call: host rasters
+  in, host maps out, the copies inside the timed region.
+* ``fp64``: the plain FP64 Jacobi-PCG GPU path on the same workload; ``fp32_over_fp64`` their ratio;
+  ``max_rel_err_vs_fp64``: max relative difference of the cumulative currents of the two solves (cells above
+  1e-12 of the maximum).
+* ``cpu_baseline``: the reference's own driver (oracle/_ref, else the C restatement) on the host cores, on a
+  bounded sample of the targets (rank 0, N = 1).
+
+``--impl reference`` times that CPU reference alone, each step a bounded sample.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Omniscape windows/s: batched FP32+refine vs plain FP64 GPU, at <=1e-6 rel err"
+WORKLOAD = {"workload": "omni_1024", "raster": "1024x1024", "radius": 32, "block_size": 3, "buffer": 0,
+            "neighbours": 8, "edge_weights": "average", "outputs": "cum_currmap"}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------------------------------------------
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Dist:
+    """Process group plumbing: barrier and max over ranks (no collective on the data path)."""
+
+    def __init__(self, world, backend):
+        self.world = world
+        self.pg = None
+        if world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=300))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+        dev = "cuda" if self.pg.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------------------------------------------
+
+class Clocks:
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------------------------------
+# the CPU reference (bounded sample)
+# ---------------------------------------------------------------------------------------------------------------
+
+def cpu_sample(r, s, kw, target_windows=1000):
+    """Sources kept only in a central square, grown until it holds about `target_windows` targets."""
+    import oracle
+    ny, nx = r.shape
+    bs = kw["block_size"]
+    side = 2 * bs
+    while True:
+        y0, x0 = (ny - side) // 2, (nx - side) // 2
+        ss = np.zeros_like(s)
+        ss[y0:y0 + side, x0:x0 + side] = s[y0:y0 + side, x0:x0 + side]
+        n = oracle.count_targets(ss, kw["radius"], kw["buffer"], bs)
+        if n >= target_windows or side >= min(nx, ny):
+            break
+        side = min(min(nx, ny), int(side * 1.25) + bs)
+    return ss, n, f"targets of the central {side}x{side} cells of the map ({n} windows, sources outside zeroed)"
+
+
+def run_cpu_reference(r, s, kw, threads):
+    import oracle
+    kind = "reference" if oracle.REF_AVAILABLE else "port"
+    t0 = time.perf_counter()
+    out = oracle.core_omniscape(r, s, kw["radius"], kw["buffer"], kw["block_size"], False, False, True, False,
+                                threads=threads, impl="ref" if kind == "reference" else "port")
+    dt = time.perf_counter() - t0
+    return dt, out["n_targets"], kind
+
+
+# ---------------------------------------------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------------------------------------------
+
+def max_rel(ours, want):
+    top = np.nanmax(np.abs(want))
+    m = ~np.isnan(want) & (np.abs(want) > 1e-12 * top)
+    return float(np.max(np.abs(ours[m] - want[m]) / np.abs(want[m]))) if m.any() else 0.0
+
+
+def time_device(lsb_om, rt, st, params, steps, warmup, flush):
+    """Per-step device times (CUDA events on the caller's stream, which waits for the call's stream)."""
+    import torch
+    for _ in range(warmup):
+        lsb_om.run_device(rt, st, params, want_stats=False)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        lsb_om.run_device(rt, st, params, want_stats=False)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+    return times
+
+
+def kernel_time(lsb_om, rt, st, params, flush, reps=3):
+    """Duration of the window kernels alone (CUDA events on the stream they are launched on), best of reps."""
+    import torch
+    from landschaft_b200 import _native as N
+    p = N.Params.from_buffer_copy(params)
+    p.use_graph = 0
+    durs = []
+    stats = None
+    for _ in range(reps):
+        flush.zero_()
+        _, stats, kt = lsb_om.run_device(rt, st, p, time_windows=True)
+        durs.append(kt)
+    torch.cuda.synchronize()
+    return min(durs), stats
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--workload", default="omni_1024")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+    from landschaft_b200 import synthetic
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        r, s, kw = synthetic.omni_1024(0)
+        ss, n, sample = cpu_sample(r, s, kw, target_windows=1000)
+        threads = os.cpu_count() or 1
+        times = []
+        kind = None
+        for i in range(args.warmup + args.steps):
+            dt, nt, kind = run_cpu_reference(r, ss, kw, threads)
+            if i >= args.warmup:
+                times.append(dt)
+        v = n / statistics.mean(times)
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "windows/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded Gaussian random field; no dataset is published for this path)",
+                "config": {**WORKLOAD, "precision": "fp64 direct (CPU)"},
+                "cpu_baseline": {"value": v, "unit": "windows/s", "cores": threads, "kind": kind, "sample": sample},
+                "e2e": {"value": v, "unit": "windows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    d = Dist(world, "nccl")
+    import landschaft_b200 as lsb
+    from landschaft_b200 import omni as lsb_om
+
+    r, s, kw = synthetic.WORKLOADS[args.workload](rank)
+    dev = torch.device("cuda", local)
+    rt = torch.from_numpy(r).to(dev)
+    st = torch.from_numpy(s).to(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # 256 MiB > 126 MB L2
+    p32 = lsb_om.make_params(kw["radius"], kw["buffer"], kw["block_size"], solver="fp32-refine")
+    p64 = lsb_om.make_params(kw["radius"], kw["buffer"], kw["block_size"], solver="fp64", preconditioner="jacobi")
+    # correctness and counts (outside the timed region)
+    out32, stats32 = lsb_om.run_device(rt, st, p32)
+    c32 = out32["current"].cpu().numpy()
+    out64, stats64 = lsb_om.run_device(rt, st, p64)
+    c64 = out64["current"].cpu().numpy()
+    n_windows = int(stats32.n_targets)
+    err = max_rel(c32, c64)
+    lsb_om.run_device(rt, st, p32)
+    launches = int(lsb_om.last_launch_count())
+
+    # device-resident timing, FP32 + refinement
+    clocks = Clocks(local)
+    d.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t32 = time_device(lsb_om, rt, st, p32, args.steps, args.warmup, flush)
+    clk = clocks.stop()
+    d.barrier()
+    torch.cuda.synchronize()
+    T32 = d.max(sum(t32))
+    value = world * n_windows * args.steps / T32
+    # plain FP64
+    t64 = time_device(lsb_om, rt, st, p64, max(1, min(args.steps, 3)), 1, flush)
+    T64 = d.max(sum(t64) / len(t64))
+    fp64_value = world * n_windows / T64
+    # e2e through the drop-in call (host numpy in, host maps out)
+    for _ in range(max(1, args.warmup)):
+        lsb.omniscape(r, kw["radius"], source=s, block_size=kw["block_size"], mask_nodata=False)
+    torch.cuda.synchronize()
+    d.barrier()
+    te = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        lsb.omniscape(r, kw["radius"], source=s, block_size=kw["block_size"], mask_nodata=False)
+        te.append(time.perf_counter() - t0)
+    TE = d.max(sum(te))
+    e2e = world * n_windows * args.steps / TE
+    # window-kernel time and roofline (rank-local)
+    ktime, kstats = kernel_time(lsb_om, rt, st, p32, flush)
+    active = lsb_om.active_blocks(s, kw["block_size"])
+    assert int(active.sum()) == n_windows
+    cells = lsb_om.window_cells(r.shape, {**kw, "active": active})  # sum over targets of the window box cells
+    hbm_bytes = cells * 24.0  # per window cell: resistance 8 + source 8 read, current 8 written
+    peak, peak_kind = peaks()
+    achieved = hbm_bytes / ktime / 1e9
+    prof = ROOT / "profiles" / "k_windows_omni_1024_traffic.json"
+    traffic = json.loads(prof.read_text())["dram_bytes_per_launch"] if prof.exists() else None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        ss, n, sample = cpu_sample(r, s, kw, target_windows=1000)
+        threads = os.cpu_count() or 1
+        dt, nt, kind = run_cpu_reference(r, ss, kw, threads)
+        cpu = {"value": n / dt, "unit": "windows/s", "cores": threads, "kind": kind, "sample": sample}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "windows/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * T32 / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32 CG + f64 refinement",
+                "data": "synthetic (seeded Gaussian random field per rank; no dataset is published for this path)",
+                "config": {**WORKLOAD, "windows_per_rank": n_windows, "parallelism": f"{world} independent rasters",
+                           "l2": "flushed between timed steps (256 MiB write)", "tol": 1e-12,
+                           "preconditioner": "multigrid V(1,1)"},
+                "e2e": {"value": e2e, "unit": "windows/s", "h2d_bytes_per_step": int(r.nbytes + s.nbytes),
+                        "d2h_bytes_per_step": int(r.nbytes)},
+                "fp64": {"value": fp64_value, "unit": "windows/s", "preconditioner": "jacobi",
+                         "ms_per_step": 1e3 * T64},
+                "fp32_over_fp64": value / fp64_value,
+                "max_rel_err_vs_fp64": err,
+                "cg_iterations": {"fp32_mean": stats32.iters_total / max(stats32.n_solved, 1),
+                                  "fp32_max": stats32.iters_max, "refine_max": stats32.refine_max,
+                                  "fp64_mean": stats64.iters_total / max(stats64.n_solved, 1),
+                                  "fp64_max": stats64.iters_max},
+                "cells_per_s": world * cells * args.steps / T32,
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                             "kernel": "k_windows", "kernel_ms": ktime * 1e3,
+                             "note": "algorithmic HBM bytes (24 B per window cell) over the window kernel's "
+                                     "event time; the solve itself runs out of shared memory"},
+                "clocks": clk, "gpu_launches": launches * args.steps, "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    d.close()
+
+
+if __name__ == "__main__":
+    main()

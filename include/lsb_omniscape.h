@@ -84,7 +84,7 @@ typedef struct lsb_omni_params {
     int32_t preconditioner; /* lsb_preconditioner */
     double tol;             /* relative FP64 residual ||b - A x|| / ||b|| at which a window is solved */
     int32_t max_iter;       /* cap on CG iterations per window (all refinement steps together) */
-    int32_t threads_per_window; /* 0: autotuned; else 256, 512 or 1024 */
+    int32_t threads_per_window; /* 0: chosen from the window size; else 256 or 512 */
     int32_t use_graph;      /* 1: capture the call's launches in a CUDA graph and replay it on repeat calls */
     int32_t mask_nodata;    /* 1: NaN on NoData cells of the outputs (Python's mask_nodata) */
 } lsb_omni_params;
@@ -101,6 +101,7 @@ typedef struct lsb_omni_stats {
     int32_t preconditioner;
     int32_t pad_;
     double worst_residual;  /* largest final relative FP64 residual */
+    double window_ms;       /* device time of the window-solve kernels (see lsb_time_window_kernels) */
 } lsb_omni_stats;
 
 /* Fill the defaults: radius 0, buffer 0, block 1, average weights, correction
@@ -147,8 +148,12 @@ int lsb_omniscape_grad(const double *resistance, const double *source, const dou
 /* Device bytes lsb_omniscape_grad needs. */
 int lsb_omniscape_grad_workspace_size(int64_t nx, int64_t ny, const lsb_omni_params *p, size_t *bytes);
 
-/* Number of kernel launches the last call on this thread enqueued (0 when replayed from a graph: 1 graph). */
+/* Number of kernels the last call on this thread launched (from a graph replay: the graph's kernel nodes). */
 int64_t lsb_last_launch_count(void);
+
+/* On this thread, record CUDA events around the window-solve kernels of calls that run without a graph and
+ * return stats: their device time goes to stats->window_ms (profiling aid; 0 = off, the default). */
+void lsb_time_window_kernels(int32_t on);
 
 /* Library version string. */
 const char *lsb_version(void);

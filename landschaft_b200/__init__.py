@@ -5,7 +5,7 @@ outputs); the windows are solved by hand-written sm_100a CUDA behind the C ABI
 of ``include/lsb_omniscape.h``.
 """
 
-from .omniscape import (  # noqa: F401
+from .omni import (  # noqa: F401
     Dataset,
     make_params,
     omniscape,

@@ -19,7 +19,8 @@ EDGE_AVERAGE, EDGE_SERIES = 0, 1
 
 # Every symbol the header declares (the CPU test checks the library exports them).
 EXPORTS = ("lsb_params_default", "lsb_omniscape_workspace_size", "lsb_omniscape", "lsb_omniscape_correction",
-           "lsb_omniscape_grad", "lsb_omniscape_grad_workspace_size", "lsb_last_launch_count", "lsb_version")
+           "lsb_omniscape_grad", "lsb_omniscape_grad_workspace_size", "lsb_last_launch_count",
+           "lsb_time_window_kernels", "lsb_version")
 
 
 class Condition(C.Structure):
@@ -41,7 +42,7 @@ class Stats(C.Structure):
     _fields_ = [("n_targets", C.c_int64), ("n_solved", C.c_int64), ("n_failed", C.c_int64),
                 ("iters_total", C.c_int64), ("iters_max", C.c_int32), ("refine_max", C.c_int32),
                 ("batches", C.c_int32), ("threads_per_window", C.c_int32), ("preconditioner", C.c_int32),
-                ("pad_", C.c_int32), ("worst_residual", C.c_double)]
+                ("pad_", C.c_int32), ("worst_residual", C.c_double), ("window_ms", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad_"}
@@ -85,6 +86,8 @@ def load():
         lib.lsb_omniscape_grad_workspace_size.restype = C.c_int
         lib.lsb_last_launch_count.argtypes = []
         lib.lsb_last_launch_count.restype = i64
+        lib.lsb_time_window_kernels.argtypes = [C.c_int32]
+        lib.lsb_time_window_kernels.restype = None
         lib.lsb_version.argtypes = []
         lib.lsb_version.restype = C.c_char_p
         _lib = lib

@@ -23,6 +23,7 @@ namespace lsb {
 namespace {
 
 thread_local int64_t g_launches = 0;
+thread_local bool g_time_windows = false;
 
 void set_err(char *err, size_t len, const char *fmt, ...) {
     if (!err || len == 0) return;
@@ -129,9 +130,9 @@ Variant choose_variant(const lsb_omni_params *p, const Geom &g) {
     if (pc == LSB_PC_AUTO) pc = v.dbl ? LSB_PC_JACOBI : LSB_PC_MG;
     v.mg = pc == LSB_PC_MG;
     int nt = p->threads_per_window;
-    if (nt != 256 && nt != 512 && nt != 1024) {
+    if (nt != 256 && nt != 512) {
         const int np = (g.W + 2) * (g.W + 2);
-        nt = np <= 1200 ? 256 : np <= 3000 ? 512 : 1024;
+        nt = np <= 1200 ? 256 : 512;
     }
     v.nt = nt;
     return v;
@@ -143,7 +144,7 @@ int resolved_pc(const lsb_omni_params *p) {
     return pc;
 }
 
-constexpr size_t kStaticSmem = 128 * 8 + 64 * 4 + 2 * kMaxLevels * 4 + 64;
+constexpr size_t kStaticSmem = 2048;  // the window kernel's static shared memory, with room to spare
 
 ArenaLayout make_layout(const Variant &v, int W, size_t smem_budget) {
     ArenaLayout L;
@@ -200,14 +201,7 @@ ArenaLayout make_layout(const Variant &v, int W, size_t smem_budget) {
 // Kernel dispatch.
 // ---------------------------------------------------------------------------
 KernelFn pick(const Variant &v) {
-    switch (v.nt) {
-        case 256:
-            return pick_windows_256(v.four, v.dbl, v.mg);
-        case 512:
-            return pick_windows_512(v.four, v.dbl, v.mg);
-        default:
-            return pick_windows_1024(v.four, v.dbl, v.mg);
-    }
+    return v.nt == 256 ? pick_windows_256(v.four, v.dbl, v.mg) : pick_windows_512(v.four, v.dbl, v.mg);
 }
 
 struct DeviceInfo {
@@ -242,7 +236,7 @@ struct Plan {
     int nparts;         // scan blocks
     // workspace offsets
     size_t o_amps, o_tindex, o_targets, o_part, o_count, o_queue, o_err, o_stat, o_condv, o_corr, o_corrwin,
-        o_corrstat, o_cur, o_fp, o_gs, o_devstats, total;
+        o_corrstat, o_cur, o_fp, o_gs, o_devstats, o_timers, total;
 };
 
 int make_plan(int64_t nx, int64_t ny, const lsb_omni_params *p, Plan *pl, char *err, size_t errlen) {
@@ -294,6 +288,7 @@ int make_plan(int64_t nx, int64_t ny, const lsb_omni_params *p, Plan *pl, char *
     pl->o_fp = take(g.fp ? static_cast<size_t>(batch) * g.W * g.W * 8 : 0);
     pl->o_gs = take(static_cast<size_t>(pl->grid) * pl->lay.gmem_bytes);
     pl->o_devstats = take(sizeof(DevStats));
+    pl->o_timers = take(sizeof(unsigned long long) * 32);
     pl->total = o;
     return LSB_OK;
 }
@@ -334,7 +329,7 @@ constexpr size_t kMaxGraphs = 16;
 // The launch sequence.
 // ---------------------------------------------------------------------------
 int enqueue(const Plan &pl, const double *res, const double *src, const lsb_omni_params *p, double *cur, double *fpm,
-            double *norm, char *ws, cudaStream_t s, char *err, size_t errlen) {
+            double *norm, char *ws, cudaStream_t s, char *err, size_t errlen, cudaEvent_t *ev = nullptr) {
     const Geom &g = pl.g;
     const int64_t n = g.nx * g.ny;
     int64_t launches = 0;
@@ -391,6 +386,10 @@ int enqueue(const Plan &pl, const double *res, const double *src, const lsb_omni
     a.corr = g.correct ? reinterpret_cast<const double *>(ws + pl.o_corr) : nullptr;
     a.gscratch = ws + pl.o_gs;
     a.lay = pl.lay;
+#ifdef LSB_PHASE_TIMERS
+    a.timers = reinterpret_cast<unsigned long long *>(ws + pl.o_timers);
+    LSB_CK(cudaMemsetAsync(a.timers, 0, sizeof(unsigned long long) * 32, s));
+#endif
     a.sp = solve_params(p);
     if (g.conditions && g.NL > 0) {
         k_block_cond<<<static_cast<int>((g.NL + 127) / 128), 128, 0, s>>>(
@@ -425,7 +424,9 @@ int enqueue(const Plan &pl, const double *res, const double *src, const lsb_omni
     for (int b = 0; b < pl.nbatches && g.NL > 0; ++b) {
         a.batch_start = static_cast<int>(b * pl.batch);
         a.queue = queue + b;
+        if (ev) LSB_CK(cudaEventRecord(ev[2 * b], s));
         pl.kern<<<pl.grid, pl.v.nt, pl.lay.smem_bytes, s>>>(a);
+        if (ev) LSB_CK(cudaEventRecord(ev[2 * b + 1], s));
         k_gather<<<gg, kGatherTX * kGatherTY, 0, s>>>(a, tindex, cur, g.fp ? fpm : nullptr);
         launches += 2;
         LSB_CK(cudaGetLastError());
@@ -548,8 +549,14 @@ int lsb_omniscape(const double *resistance, const double *source, int64_t nx, in
         g_launches = launches;
         graphed = true;
     }
+    std::vector<cudaEvent_t> ev;
     if (!graphed) {
-        rc = enqueue(pl, resistance, source, p, current, flow_potential, normalized, ws, s, err, errlen);
+        if (stats && g_time_windows) {
+            ev.resize(2 * static_cast<size_t>(pl.nbatches));
+            for (auto &e : ev) LSB_CK(cudaEventCreate(&e));
+        }
+        rc = enqueue(pl, resistance, source, p, current, flow_potential, normalized, ws, s, err, errlen,
+                     ev.empty() ? nullptr : ev.data());
         if (rc) return rc;
     }
     if (stats) {
@@ -559,6 +566,29 @@ int lsb_omniscape(const double *resistance, const double *source, int64_t nx, in
         LSB_CK(cudaMemcpyAsync(&hdr[0], ws + pl.o_count, 4, cudaMemcpyDeviceToHost, s));
         LSB_CK(cudaMemcpyAsync(&hdr[1], ws + pl.o_err, 4, cudaMemcpyDeviceToHost, s));
         LSB_CK(cudaStreamSynchronize(s));
+        stats->window_ms = 0.0;
+        for (size_t b = 0; b + 1 < ev.size(); b += 2) {
+            float ms = 0.f;
+            if (hdr[0] > static_cast<int>(b / 2 * pl.batch) && cudaEventElapsedTime(&ms, ev[b], ev[b + 1]) == cudaSuccess)
+                stats->window_ms += ms;
+        }
+        for (auto &e : ev) cudaEventDestroy(e);
+        ev.clear();
+#ifdef LSB_PHASE_TIMERS
+        {
+            unsigned long long tm[PH_COUNT];
+            LSB_CK(cudaMemcpy(tm, ws + pl.o_timers, sizeof tm, cudaMemcpyDeviceToHost));
+            static const char *names[PH_COUNT] = {"load", "flood", "mark", "assemble", "mg_setup", "resid64",
+                                                  "cg", "vcycle", "currents", "other"};
+            double tot = 0;
+            for (int k = 0; k < PH_COUNT; ++k) tot += static_cast<double>(tm[k]);
+            fprintf(stderr, "[phases] windows=%d cycles/window:", hdr[0]);
+            for (int k = 0; k < PH_COUNT; ++k)
+                fprintf(stderr, " %s=%.0f(%.0f%%)", names[k], tm[k] / std::max(1.0, static_cast<double>(hdr[0])),
+                        100.0 * tm[k] / std::max(tot, 1.0));
+            fprintf(stderr, "\n");
+        }
+#endif
         stats->n_targets = hdr[0];
         stats->n_solved = ds.n_solved;
         stats->n_failed = ds.n_failed;
@@ -657,6 +687,8 @@ int lsb_omniscape_grad(const double *, const double *, const double *, int64_t, 
 }
 
 int64_t lsb_last_launch_count(void) { return g_launches; }
+
+void lsb_time_window_kernels(int32_t on) { g_time_windows = on != 0; }
 
 const char *lsb_version(void) { return "landschaft_b200 0.1 (sm_100a)"; }
 

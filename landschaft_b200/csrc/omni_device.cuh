@@ -136,6 +136,7 @@ struct WinStat {
 // ---------------------------------------------------------------------------
 template <int NT>
 struct Reducer {
+    static constexpr int NW = NT / 32;
     double *red;
     int slot;
     __device__ __forceinline__ double *next() {
@@ -143,76 +144,68 @@ struct Reducer {
         ++slot;
         return b;
     }
+    // Lane 0 of every warp holds its warp's value; after the barrier each warp
+    // sums the partials with the same shuffle tree (the same order in every
+    // warp) and broadcasts lane 0's result.
+    __device__ __forceinline__ static double tree_sum(double v) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        return __shfl_sync(0xffffffffu, v, 0);
+    }
+    __device__ __forceinline__ static double tree_max(double v) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+        return __shfl_sync(0xffffffffu, v, 0);
+    }
     __device__ __forceinline__ double sum(double v) {
-        constexpr int NW = NT / 32;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
         double *b = next();
-        if ((threadIdx.x & 31) == 0) b[threadIdx.x >> 5] = v;
+        const int lane = threadIdx.x & 31;
+        if (lane == 0) b[threadIdx.x >> 5] = v;
         __syncthreads();
-        double s = 0.0;
-#pragma unroll
-        for (int k = 0; k < NW; ++k) s += b[k];
-        return s;
+        return tree_sum(lane < NW ? b[lane] : 0.0);
     }
     __device__ __forceinline__ void sum2(double &a, double &c) {
-        constexpr int NW = NT / 32;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             a += __shfl_down_sync(0xffffffffu, a, o);
             c += __shfl_down_sync(0xffffffffu, c, o);
         }
         double *b = next();
-        if ((threadIdx.x & 31) == 0) {
+        const int lane = threadIdx.x & 31;
+        if (lane == 0) {
             b[threadIdx.x >> 5] = a;
             b[32 + (threadIdx.x >> 5)] = c;
         }
         __syncthreads();
-        double s = 0.0, t = 0.0;
-#pragma unroll
-        for (int k = 0; k < NW; ++k) {
-            s += b[k];
-            t += b[32 + k];
-        }
-        a = s;
-        c = t;
+        a = tree_sum(lane < NW ? b[lane] : 0.0);
+        c = tree_sum(lane < NW ? b[32 + lane] : 0.0);
     }
     __device__ __forceinline__ double max(double v) {
-        constexpr int NW = NT / 32;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
         double *b = next();
-        if ((threadIdx.x & 31) == 0) b[threadIdx.x >> 5] = v;
+        const int lane = threadIdx.x & 31;
+        if (lane == 0) b[threadIdx.x >> 5] = v;
         __syncthreads();
-        double s = b[0];
-#pragma unroll
-        for (int k = 1; k < NW; ++k) s = fmax(s, b[k]);
-        return s;
+        return tree_max(lane < NW ? b[lane] : -1.0 / 0.0);
     }
     __device__ __forceinline__ void max2(double &a, double &c) {
-        constexpr int NW = NT / 32;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             a = fmax(a, __shfl_down_sync(0xffffffffu, a, o));
             c = fmax(c, __shfl_down_sync(0xffffffffu, c, o));
         }
         double *b = next();
-        if ((threadIdx.x & 31) == 0) {
+        const int lane = threadIdx.x & 31;
+        if (lane == 0) {
             b[threadIdx.x >> 5] = a;
             b[32 + (threadIdx.x >> 5)] = c;
         }
         __syncthreads();
-        double s = b[0], t = b[32];
-#pragma unroll
-        for (int k = 1; k < NW; ++k) {
-            s = fmax(s, b[k]);
-            t = fmax(t, b[32 + k]);
-        }
-        a = s;
-        c = t;
-    }
-    __device__ __forceinline__ int count(int v) {  // block-wide integer sum (exact)
-        return static_cast<int>(sum(static_cast<double>(v)));
+        a = tree_max(lane < NW ? b[lane] : -1.0 / 0.0);
+        c = tree_max(lane < NW ? b[32 + lane] : -1.0 / 0.0);
     }
 };
 

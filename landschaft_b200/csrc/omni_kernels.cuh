@@ -244,7 +244,8 @@ __global__ void __launch_bounds__(kGatherTX *kGatherTY) k_gather(const KArgs a, 
     auto lo = [&](int64_t c) { const int64_t v = c - D - br; return v <= 0 ? int64_t(0) : (v + bs - 1) / bs; };
     auto hi = [&](int64_t c, int nb) { const int64_t v = (c + D - br); if (v < 0) return int64_t(-1); const int64_t k = v / bs; return k < nb - 1 ? k : int64_t(nb - 1); };
     const int64_t ix0 = lo(X0), ix1 = hi(X1, a.nbx), iy0 = lo(Y0), iy1 = hi(Y1, a.nby);
-    double c = 0.0, f = 0.0;
+    // each window is added to the running map value in target order, so that batches do not change the bits
+    double c = in ? cum[Y * a.nx + X] : 0.0, f = (in && fpmap) ? fpmap[Y * a.nx + X] : 0.0;
     for (int64_t ix = ix0; ix <= ix1; ++ix) {
         const int64_t tx = br + ix * bs;
         const int64_t x0 = tx - D > 0 ? tx - D : 0, x1 = tx + D < a.nx - 1 ? tx + D : a.nx - 1;
@@ -261,8 +262,8 @@ __global__ void __launch_bounds__(kGatherTX *kGatherTY) k_gather(const KArgs a, 
         }
     }
     if (in) {
-        cum[Y * a.nx + X] += c;
-        if (fpmap) fpmap[Y * a.nx + X] += f;
+        cum[Y * a.nx + X] = c;
+        if (fpmap) fpmap[Y * a.nx + X] = f;
     }
 }
 

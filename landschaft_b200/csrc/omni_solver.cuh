@@ -41,7 +41,13 @@ struct KArgs {
     double n_corr_sources;  // cells within radius of the correction disk (mode 1)
     // adjoint (mode 2): weights of J on the map; per-window gradient slots
     const double *weight;
+    // per-phase cycle counters (builds with LSB_PHASE_TIMERS only)
+    unsigned long long *timers;
 };
+
+// Phases of a window solve, for the cycle counters of profiling builds.
+enum Phase : int { PH_LOAD = 0, PH_FLOOD, PH_MARK, PH_ASSEMBLE, PH_MG_SETUP, PH_RESID, PH_CG, PH_VCYCLE, PH_CURRENTS,
+                   PH_OTHER, PH_COUNT };
 
 template <typename X>
 __device__ __forceinline__ X *arena_ptr(const ArenaLayout &L, int a, char *sm, char *gm) {
@@ -69,7 +75,7 @@ __device__ __forceinline__ double tmax(double a, double b) { return fmax(a, b); 
 // Block-wide ordered compaction of flags over [0, n): out[k] = i of the k-th
 // flagged i (increasing).  Returns the count.  scan: shared, >= 33 ints.
 template <int NT, typename F>
-__device__ int block_compact(int n, F flag, uint16_t *out, int *scan) {
+__device__ __forceinline__ int block_compact(int n, F flag, uint16_t *out, int *scan) {
     constexpr int NW = NT / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int base = 0;
@@ -106,12 +112,32 @@ struct Win {
     Reducer<NT> &red;
     int *scan;       // shared scratch (>= 64 ints)
     int *lvh, *lvw;  // shared: level dimensions
+    short *cidx;     // shared: padded indices of the coarsest level's cells (kNcMax)
+    float invP = 1.f;  // 1 / G.P
     WinGeom G;
     int nu = 0;      // number of unknowns
     int nlev = 1;
+#ifdef LSB_PHASE_TIMERS
+    unsigned long long *tacc = nullptr;  // shared, PH_COUNT + 1 (the last: time of the previous mark)
+#endif
 
-    __device__ Win(const KArgs &a_, char *sm_, char *gm_, Reducer<NT> &red_, int *scan_, int *lvh_, int *lvw_)
-        : a(a_), sm(sm_), gm(gm_), red(red_), scan(scan_), lvh(lvh_), lvw(lvw_) {}
+    // Profiling builds: charge the time since the previous mark to phase k (a barrier first).
+    __device__ __forceinline__ void mark(int k) {
+#ifdef LSB_PHASE_TIMERS
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const unsigned long long t = clock64();
+            tacc[k] += t - tacc[PH_COUNT];
+            tacc[PH_COUNT] = t;
+        }
+#else
+        (void)k;
+#endif
+    }
+
+    __device__ Win(const KArgs &a_, char *sm_, char *gm_, Reducer<NT> &red_, int *scan_, int *lvh_, int *lvw_,
+                   short *cidx_)
+        : a(a_), sm(sm_), gm(gm_), red(red_), scan(scan_), lvh(lvh_), lvw(lvw_), cidx(cidx_) {}
 
     template <typename X>
     __device__ __forceinline__ X *A(int k) const { return arena_ptr<X>(a.lay, k, sm, gm); }
@@ -125,11 +151,12 @@ struct Win {
     // Conductance, candidates and raw sources (omniscape.cpp:495-519).  FLOW
     // keeps the sources the LAND pass scaled.  Returns the sum of positive raw
     // sources (the scaling denominator; 0 for FLOW).
-    __device__ double load(int kind, double amps) {
+    __device__ __forceinline__ double load(int kind, double amps) {
         uint8_t *mask = A<uint8_t>(AR_MASK);
         double *g64 = A<double>(AR_G64), *x64 = A<double>(AR_X64), *b64 = A<double>(AR_B64);
         const int h = G.h, w = G.w, P = G.P, NP = G.NP;
         const int R = a.R, D = a.D, br = a.br;
+        invP = 1.0f / static_cast<float>(P);
         const int64_t ylim = (D + br < a.ny - 1 ? D + br : a.ny - 1), xlim = (D + br < a.nx - 1 ? D + br : a.nx - 1);
         double pos = 0.0;
         for (int i = threadIdx.x; i < NP; i += NT) {
@@ -191,7 +218,7 @@ struct Win {
     }
 
     // Conditions (omniscape.cpp:526-530, match_condition :218-230).
-    __device__ void apply_conditions(double v1, double v2) {
+    __device__ __forceinline__ void apply_conditions(double v1, double v2) {
         double *b64 = A<double>(AR_B64);
         for (int k = 0; k < 2; ++k) {
             const double *c = a.cond_present[k];
@@ -217,7 +244,7 @@ struct Win {
     // Monotone label propagation until no cell changes; bounded by the number
     // of cells (every productive sweep adds one).  Returns false when the
     // ground has no node.
-    __device__ bool flood(int kind) {
+    __device__ __forceinline__ bool flood(int kind) {
         uint8_t *mask = A<uint8_t>(AR_MASK);
         const int ground = (G.gy + 1) * G.P + G.gx + 1;
         if (kind == KIND_FLOW) {
@@ -255,7 +282,7 @@ struct Win {
 
     // Sum of the sources over the unknowns-to-be (omniscape.cpp:101, 149-150);
     // marks the unknowns and lists them.
-    __device__ double mark_unknowns() {
+    __device__ __forceinline__ double mark_unknowns() {
         uint8_t *mask = A<uint8_t>(AR_MASK);
         const double *b64 = A<double>(AR_B64);
         const int ground = (G.gy + 1) * G.P + G.gx + 1;
@@ -276,7 +303,7 @@ struct Win {
     // ---- 3. assembly -------------------------------------------------------
     // Diagonal summed in column-major neighbour order with the 10 eps shift
     // (system.cpp:458-487); stencil conductances with sentinels off the nodes.
-    __device__ void assemble() {
+    __device__ __forceinline__ void assemble() {
         const uint8_t *mask = A<uint8_t>(AR_MASK);
         const double *g64 = A<double>(AR_G64);
         T *gT = A<T>(AR_GT), *invd = A<T>(AR_INVD), *z = A<T>(AR_Z);
@@ -386,7 +413,112 @@ struct Win {
     }
 
     // ---- multigrid set-up (Galerkin R A P, masked bilinear P) -------------
-    __device__ void mg_setup() {
+    // Coarse point J of a coarsened dimension sits on fine point 2J; a fine
+    // point's weight in P is 1 on its coarse point and 1/2 next to one.  P's
+    // rows of fine cells that are not unknowns (level 0) or not active are
+    // zero, so coarse cells whose support holds no such cell are inactive
+    // (identity rows).  Coarse operators are 9-point; each cell stores its
+    // diagonal and the 4 entries towards E, SW, S, SE (the rest by symmetry).
+
+    // Cells of level l, warps along rows and lanes along columns (no division).
+    template <class F>
+    __device__ __forceinline__ void for_cells(int l, F f) const {
+        const int h = lvh[l], w = lvw[l], P = w + 2;
+        for (int y = threadIdx.x >> 5; y < h; y += NT / 32)
+            for (int x = threadIdx.x & 31; x < w; x += 32) f(y, x, (y + 1) * P + x + 1);
+    }
+
+    // Level l -> l + 1 at coarse cell (jy, jx) when both dimensions coarsen:
+    // all but the entries resolved at compile time.
+    template <int L0>
+    __device__ __forceinline__ void rap_cell(int l, int jy, int jx, T (&acc)[5], bool &act) const {
+        const int hf = lvh[l], wf = lvw[l], Pf = wf + 2;
+#pragma unroll
+        for (int ay = -1; ay <= 1; ++ay) {
+#pragma unroll
+            for (int ax = -1; ax <= 1; ++ax) {
+                const int fy = 2 * jy + ay, fx = 2 * jx + ax;
+                if (fy < 0 || fy >= hf || fx < 0 || fx >= wf) continue;
+                const int i = (fy + 1) * Pf + fx + 1;
+                if (!(L0 ? (A<uint8_t>(AR_MASK)[i] & M_UNKNOWN) != 0 : LV<T>(l, LV_INVD)[i] != T(0))) continue;
+                act = true;
+                const T wi = (ay == 0 ? T(1) : T(0.5)) * (ax == 0 ? T(1) : T(0.5));
+#pragma unroll
+                for (int sy = -1; sy <= 1; ++sy) {
+#pragma unroll
+                    for (int sx = -1; sx <= 1; ++sx) {
+                        if (FOUR && L0 && sy != 0 && sx != 0) continue;
+                        const T v = wi * (L0 ? entry0(i, sy, sx) : entryc(l, i, sy, sx));
+                        const int dy = ay + sy, dx = ax + sx;  // fine j relative to 2J, in [-2, 2]
+#pragma unroll
+                        for (int py = 0; py < 2; ++py) {
+#pragma unroll
+                            for (int px = 0; px < 2; ++px) {
+                                const bool oy = (dy & 1) != 0, ox = (dx & 1) != 0;
+                                if ((!oy && py) || (!ox && px)) continue;
+                                const int ky = oy ? (dy - 1) / 2 + py : dy / 2;
+                                const int kx = ox ? (dx - 1) / 2 + px : dx / 2;
+                                const int slot = (ky == 0 && kx == 0)    ? 0
+                                                 : (ky == 0 && kx == 1)  ? 1
+                                                 : (ky == 1 && kx == -1) ? 2
+                                                 : (ky == 1 && kx == 0)  ? 3
+                                                 : (ky == 1 && kx == 1)  ? 4
+                                                                         : -1;
+                                if (slot < 0) continue;
+                                acc[slot] += v * (oy ? T(0.5) : T(1)) * (ox ? T(0.5) : T(1));
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+
+    // The general case (a dimension of at most 3 cells does not coarsen).
+    __device__ __forceinline__ void rap_cell_general(int l, int jy, int jx, bool cy, bool cx, T (&acc)[5],
+                                                     bool &act) const {
+        const int hf = lvh[l], wf = lvw[l], Pf = wf + 2;
+        const int hc = lvh[l + 1], wc = lvw[l + 1];
+        for (int ay = (cy ? -1 : 0); ay <= (cy ? 1 : 0); ++ay) {
+            const int fy = cy ? 2 * jy + ay : jy;
+            if (fy < 0 || fy >= hf) continue;
+            for (int ax = (cx ? -1 : 0); ax <= (cx ? 1 : 0); ++ax) {
+                const int fx = cx ? 2 * jx + ax : jx;
+                if (fx < 0 || fx >= wf) continue;
+                const int i = (fy + 1) * Pf + fx + 1;
+                if (!active(l, i)) continue;
+                act = true;
+                const T wi = (ay == 0 ? T(1) : T(0.5)) * (ax == 0 ? T(1) : T(0.5));
+                for (int sy = -1; sy <= 1; ++sy)
+                    for (int sx = -1; sx <= 1; ++sx) {
+                        const T aij = l == 0 ? entry0(i, sy, sx) : entryc(l, i, sy, sx);
+                        if (aij == T(0)) continue;
+                        const int gy = fy + sy, gx = fx + sx;
+                        for (int e = 0; e < 5; ++e) {
+                            const int ky = jy + (e < 2 ? 0 : 1);
+                            const int kx = jx + (e == 0 ? 0 : e == 1 ? 1 : e == 2 ? -1 : e == 3 ? 0 : 1);
+                            if (ky >= hc || kx < 0 || kx >= wc) continue;
+                            T py, px;
+                            if (cy) {
+                                const int dd = gy - 2 * ky;
+                                py = dd == 0 ? T(1) : (dd == 1 || dd == -1) ? T(0.5) : T(0);
+                            } else {
+                                py = gy == ky ? T(1) : T(0);
+                            }
+                            if (cx) {
+                                const int dd = gx - 2 * kx;
+                                px = dd == 0 ? T(1) : (dd == 1 || dd == -1) ? T(0.5) : T(0);
+                            } else {
+                                px = gx == kx ? T(1) : T(0);
+                            }
+                            acc[e] += wi * aij * py * px;
+                        }
+                    }
+            }
+        }
+    }
+
+    __device__ __forceinline__ void mg_setup() {
         nlev = mg_levels(G.h, G.w);
         if (threadIdx.x == 0) {
             int h = G.h, w = G.w;
@@ -399,83 +531,58 @@ struct Win {
         }
         __syncthreads();
         for (int l = 1; l < nlev; ++l) {
-            const int hf = lvh[l - 1], wf = lvw[l - 1], Pf = wf + 2;
-            const int hc = lvh[l], wc = lvw[l], Pc = wc + 2, NPc = (hc + 2) * Pc;
+            const int hf = lvh[l - 1], wf = lvw[l - 1];
+            const int hc = lvh[l], wc = lvw[l], NPc = (hc + 2) * (wc + 2);
             const bool cy = hc != hf, cx = wc != wf;
             T *c0 = LV<T>(l, LV_C0), *cE = LV<T>(l, LV_CE), *cSW = LV<T>(l, LV_CSW), *cS = LV<T>(l, LV_CS),
               *cSE = LV<T>(l, LV_CSE), *iv = LV<T>(l, LV_INVD), *x = LV<T>(l, LV_X), *b = LV<T>(l, LV_B),
               *t = LV<T>(l, LV_T);
             for (int J = threadIdx.x; J < NPc; J += NT) {
-                const int jpy = J / Pc, jy = jpy - 1, jx = J - jpy * Pc - 1;
-                T acc[5] = {T(0), T(0), T(0), T(0), T(0)};
-                bool act = false;
-                if (jy >= 0 && jy < hc && jx >= 0 && jx < wc) {
-                    for (int ay = (cy ? -1 : 0); ay <= (cy ? 1 : 0); ++ay) {
-                        const int fy = cy ? 2 * jy + ay : jy;
-                        if (fy < 0 || fy >= hf) continue;
-                        const T wa = ay == 0 ? T(1) : T(0.5);
-                        for (int ax = (cx ? -1 : 0); ax <= (cx ? 1 : 0); ++ax) {
-                            const int fx = cx ? 2 * jx + ax : jx;
-                            if (fx < 0 || fx >= wf) continue;
-                            const int i = (fy + 1) * Pf + fx + 1;
-                            if (!active(l - 1, i)) continue;
-                            act = true;
-                            const T wi = wa * (ax == 0 ? T(1) : T(0.5));
-                            for (int sy = -1; sy <= 1; ++sy)
-                                for (int sx = -1; sx <= 1; ++sx) {
-                                    const T aij = l == 1 ? entry0(i, sy, sx) : entryc(l - 1, i, sy, sx);
-                                    if (aij == T(0)) continue;
-                                    const int gy = fy + sy, gx = fx + sx;  // fine j
-                                    const T base = wi * aij;
-                                    // coarse K = J + e, e in {C, E, SW, S, SE}
-#pragma unroll
-                                    for (int e = 0; e < 5; ++e) {
-                                        const int ey = e == 0 ? 0 : e == 1 ? 0 : 1;
-                                        const int ex = e == 0 ? 0 : e == 1 ? 1 : e == 2 ? -1 : e == 3 ? 0 : 1;
-                                        const int ky = jy + ey, kx = jx + ex;
-                                        if (ky >= hc || kx < 0 || kx >= wc) continue;
-                                        T py, px;
-                                        if (cy) {
-                                            const int dd = gy - 2 * ky;
-                                            py = dd == 0 ? T(1) : (dd == 1 || dd == -1) ? T(0.5) : T(0);
-                                        } else {
-                                            py = gy == ky ? T(1) : T(0);
-                                        }
-                                        if (cx) {
-                                            const int dd = gx - 2 * kx;
-                                            px = dd == 0 ? T(1) : (dd == 1 || dd == -1) ? T(0.5) : T(0);
-                                        } else {
-                                            px = gx == kx ? T(1) : T(0);
-                                        }
-                                        acc[e] += base * py * px;
-                                    }
-                                }
-                        }
-                    }
-                }
-                c0[J] = act ? acc[0] : T(0);
-                cE[J] = act ? acc[1] : T(0);
-                cSW[J] = act ? acc[2] : T(0);
-                cS[J] = act ? acc[3] : T(0);
-                cSE[J] = act ? acc[4] : T(0);
-                iv[J] = act ? static_cast<T>(a.sp.omega) / acc[0] : T(0);
+                c0[J] = T(0);
+                cE[J] = T(0);
+                cSW[J] = T(0);
+                cS[J] = T(0);
+                cSE[J] = T(0);
+                iv[J] = T(0);
                 x[J] = T(0);
                 b[J] = T(0);
                 t[J] = T(0);
             }
             __syncthreads();
-            // entries towards inactive cells were accumulated through P rows of
-            // inactive fine cells only, which are zero: nothing to clear.
+            const T om = static_cast<T>(a.sp.omega);
+            for_cells(l, [&](int jy, int jx, int J) {
+                T acc[5] = {T(0), T(0), T(0), T(0), T(0)};
+                bool act = false;
+                if (cy && cx) {
+                    if (l == 1)
+                        rap_cell<1>(0, jy, jx, acc, act);
+                    else
+                        rap_cell<0>(l - 1, jy, jx, acc, act);
+                } else {
+                    rap_cell_general(l - 1, jy, jx, cy, cx, acc, act);
+                }
+                if (!act) return;
+                // entries towards cells outside the coarse box stay zero
+                c0[J] = acc[0];
+                cE[J] = jx + 1 < wc ? acc[1] : T(0);
+                cSW[J] = (jy + 1 < hc && jx > 0) ? acc[2] : T(0);
+                cS[J] = jy + 1 < hc ? acc[3] : T(0);
+                cSE[J] = (jy + 1 < hc && jx + 1 < wc) ? acc[4] : T(0);
+                iv[J] = om / acc[0];
+            });
+            __syncthreads();
         }
         dense_setup();
     }
 
     // Pseudo-inverse of the coarsest operator (at most kNcMax cells): Cholesky
     // with skipped (near-zero) pivots, then one column of the inverse per lane.
-    __device__ void dense_setup() {
+    // Also lists the coarsest cells' padded indices (cidx).
+    __device__ __forceinline__ void dense_setup() {
         double *M = A<double>(AR_DENSE);
         const int l = nlev - 1;
         const int hc = lvh[l], wc = lvw[l], Pc = wc + 2, n = hc * wc;
+        if (threadIdx.x < n) cidx[threadIdx.x] = static_cast<short>((threadIdx.x / wc + 1) * Pc + threadIdx.x % wc + 1);
         for (int e = threadIdx.x; e < kNcMax * kNcMax; e += NT) {
             const int u = e / kNcMax, v = e - u * kNcMax;
             double val = 0.0;
@@ -496,9 +603,7 @@ struct Win {
         if (threadIdx.x < 32) {
             const int lane = threadIdx.x;
             // in-place lower Cholesky; skipped pivots get L = identity column
-            __shared__ unsigned skip_bits;
-            if (lane == 0) skip_bits = 0u;
-            __syncwarp();
+            unsigned skip_bits = 0u;
             const double od = lane < n ? M[lane * kNcMax + lane] : 0.0;  // original diagonal
             for (int k = 0; k < n; ++k) {
                 const double piv = M[k * kNcMax + k];
@@ -507,10 +612,8 @@ struct Win {
                 // dependent direction of the masked prolongation; left out of the inverse
                 const bool skip = !(piv > 1e-10 * odk);
                 if (skip) {
-                    if (lane == 0) skip_bits |= 1u << k;
-                    if (lane < n) {
-                        M[lane * kNcMax + k] = lane == k ? 1.0 : 0.0;
-                    }
+                    skip_bits |= 1u << k;
+                    if (lane < n) M[lane * kNcMax + k] = lane == k ? 1.0 : 0.0;
                     __syncwarp();
                     continue;
                 }
@@ -526,8 +629,7 @@ struct Win {
                 __syncwarp();
             }
             const unsigned sk = skip_bits;
-            // column c of the inverse, in the strictly upper triangle + a copy:
-            // solve L y = e_c, then L^T x = y, skipping skipped unknowns.
+            // column `lane` of the inverse: L y = e_lane, then L^T x = y, skipped unknowns at 0
             double col[kNcMax];
             if (lane < n) {
                 for (int i = 0; i < n; ++i) col[i] = 0.0;
@@ -552,66 +654,74 @@ struct Win {
                 }
             }
             __syncwarp();
-            // store the inverse in the upper triangle rows (i <= c): M[c][i] for i >= c is free? use
-            // the transposed store into the strictly upper part plus the diagonal, after all reads.
+            // the inverse is symmetric: row `lane`, columns >= lane (after every lane has read L)
             if (lane < n)
                 for (int i = 0; i < n; ++i)
-                    if (i >= lane) M[lane * kNcMax + i] = col[i];  // row lane, columns >= lane (symmetric)
+                    if (i >= lane) M[lane * kNcMax + i] = col[i];
         }
         __syncthreads();
     }
 
+    // Row of a padded index of level 0 (i < 65536, 3 <= P <= 256): exact in float.
+    __device__ __forceinline__ int row0(int i) const {
+        return static_cast<int>((static_cast<float>(i) + 0.5f) * invP);
+    }
+
     // z = B r: one V(1,1) cycle, damped-Jacobi smoothing, exact coarsest.
     // r is level-0 (unknowns only); the result goes to AR_Q; AR_Z is scratch.
-    __device__ void vcycle(const T *r) {
+    __device__ __forceinline__ void vcycle(const T *r) {
         const uint16_t *ul = A<uint16_t>(AR_ULIST);
         const T *gT = A<T>(AR_GT), *invd = A<T>(AR_INVD);
         T *z = A<T>(AR_Z), *q = A<T>(AR_Q);
         const T om = static_cast<T>(a.sp.omega);
-        for (int k = threadIdx.x; k < nu; k += NT) {
-            const int i = ul[k];
-            z[i] = om * invd[i] * r[i];
-        }
-        __syncthreads();
         if (nlev == 1) {
             // the window is its own coarsest level
-            coarse_solve(0, r, z);
-            __syncthreads();
-            for (int k = threadIdx.x; k < nu; k += NT) {
-                const int i = ul[k];
-                q[i] = z[i];
-            }
+            coarse_solve(0, r, q);
             __syncthreads();
             return;
         }
+        // pre-smoothing from zero and the residual in one pass: z = w D^-1 r, q = r - A z
         for (int k = threadIdx.x; k < nu; k += NT) {
             const int i = ul[k];
-            q[i] = r[i] - apply0(gT, z, i);
+            const T zi = om * invd[i] * r[i];
+            z[i] = zi;
+            q[i] = r[i] - apply0_scaled(gT, r, invd, om, i, zi);
         }
         __syncthreads();
         restrict_to(1, q);
         for (int l = 1; l < nlev - 1; ++l) {
-            const int NPc = (lvh[l] + 2) * (lvw[l] + 2);
-            T *x = LV<T>(l, LV_X), *b = LV<T>(l, LV_B), *t = LV<T>(l, LV_T);
-            const T *iv = LV<T>(l, LV_INVD);
-            for (int i = threadIdx.x; i < NPc; i += NT) x[i] = iv[i] * b[i];
-            __syncthreads();
-            for (int i = threadIdx.x; i < NPc; i += NT)
-                if (iv[i] != T(0)) t[i] = b[i] - applyc(l, x, i);
+            T *x = LV<T>(l, LV_X), *t = LV<T>(l, LV_T);
+            const T *b = LV<T>(l, LV_B), *iv = LV<T>(l, LV_INVD);
+            const int P = lvw[l] + 2;
+            const T *c0 = LV<T>(l, LV_C0), *cE = LV<T>(l, LV_CE), *cSW = LV<T>(l, LV_CSW), *cS = LV<T>(l, LV_CS),
+                    *cSE = LV<T>(l, LV_CSE);
+            for_cells(l, [&](int, int, int i) {
+                const T ivi = iv[i];
+                if (ivi == T(0)) return;
+                auto xv = [&](int j) { return iv[j] * b[j]; };
+                const T xi = ivi * b[i];
+                x[i] = xi;
+                T s = c0[i] * xi;
+                s += cE[i] * xv(i + 1) + cSW[i] * xv(i + P - 1) + cS[i] * xv(i + P) + cSE[i] * xv(i + P + 1);
+                s += cE[i - 1] * xv(i - 1) + cSW[i - P + 1] * xv(i - P + 1) + cS[i - P] * xv(i - P) +
+                     cSE[i - P - 1] * xv(i - P - 1);
+                t[i] = b[i] - s;
+            });
             __syncthreads();
             restrict_to(l + 1, t);
         }
         coarse_solve(nlev - 1, LV<T>(nlev - 1, LV_B), LV<T>(nlev - 1, LV_X));
         __syncthreads();
         for (int l = nlev - 2; l >= 1; --l) {
-            const int NPc = (lvh[l] + 2) * (lvw[l] + 2);
-            T *x = LV<T>(l, LV_X), *b = LV<T>(l, LV_B), *t = LV<T>(l, LV_T);
-            const T *iv = LV<T>(l, LV_INVD);
+            T *x = LV<T>(l, LV_X), *t = LV<T>(l, LV_T);
+            const T *b = LV<T>(l, LV_B), *iv = LV<T>(l, LV_INVD);
             const T *xc = LV<T>(l + 1, l + 1 == nlev - 1 ? LV_X : LV_T);
             prolong_add(l, x, xc);
             __syncthreads();
-            for (int i = threadIdx.x; i < NPc; i += NT)
-                if (iv[i] != T(0)) t[i] = x[i] + iv[i] * (b[i] - applyc(l, x, i));
+            for_cells(l, [&](int, int, int i) {
+                const T ivi = iv[i];
+                if (ivi != T(0)) t[i] = x[i] + ivi * (b[i] - applyc(l, x, i));
+            });
             __syncthreads();
         }
         prolong_add(0, z, LV<T>(1, nlev - 1 == 1 ? LV_X : LV_T));
@@ -623,39 +733,83 @@ struct Win {
         __syncthreads();
     }
 
-    // b_{l} = P^T t_{l-1} (level l-1 residual, zero off its active cells).
-    __device__ void restrict_to(int l, const T *tf) {
+    // (A z)_i with z_n = w invd_n r_n computed from the neighbours' r (the
+    // pre-smoothed iterate without storing it first).
+    __device__ __forceinline__ T apply0_scaled(const T *gT, const T *r, const T *invd, T om, int i, T zi) const {
+        const T gi = gT[i];
+        T ao = T(0), ad = T(0);
+        if (a.series) {
+#pragma unroll
+            for (int dd = 0; dd < ND; ++dd) {
+                const int n = i + noff(dd);
+                const T wv = T(2) / (gi + gT[n]);
+                const T zn = om * invd[n] * r[n];
+                if (NB::diag(dd))
+                    ad += wv * (zi - zn);
+                else
+                    ao += wv * (zi - zn);
+            }
+            return ao + ad * T(0.70710678118654752440);
+        }
+#pragma unroll
+        for (int dd = 0; dd < ND; ++dd) {
+            const int n = i + noff(dd);
+            const T wv = tmax(gi + gT[n], T(0));
+            const T zn = om * invd[n] * r[n];
+            if (NB::diag(dd))
+                ad += wv * (zi - zn);
+            else
+                ao += wv * (zi - zn);
+        }
+        return ao * T(0.5) + ad * T(kInvTwoSqrt2);
+    }
+
+    // b_{l} = P^T t_{l-1} (level l-1 residual, zero off its active cells); ends with a barrier.
+    __device__ __forceinline__ void restrict_to(int l, const T *tf) {
         const int hf = lvh[l - 1], wf = lvw[l - 1], Pf = wf + 2;
-        const int hc = lvh[l], wc = lvw[l], Pc = wc + 2, NPc = (hc + 2) * Pc;
+        const int hc = lvh[l], wc = lvw[l];
         const bool cy = hc != hf, cx = wc != wf;
         T *b = LV<T>(l, LV_B);
         const T *iv = LV<T>(l, LV_INVD);
-        for (int J = threadIdx.x; J < NPc; J += NT) {
-            if (iv[J] == T(0)) continue;
-            const int jpy = J / Pc, jy = jpy - 1, jx = J - jpy * Pc - 1;
-            T s = T(0);
-            for (int ay = (cy ? -1 : 0); ay <= (cy ? 1 : 0); ++ay) {
-                const int fy = cy ? 2 * jy + ay : jy;
-                if (fy < 0 || fy >= hf) continue;
-                const T wa = ay == 0 ? T(1) : T(0.5);
-                for (int ax = (cx ? -1 : 0); ax <= (cx ? 1 : 0); ++ax) {
-                    const int fx = cx ? 2 * jx + ax : jx;
-                    if (fx < 0 || fx >= wf) continue;
-                    s += wa * (ax == 0 ? T(1) : T(0.5)) * tf[(fy + 1) * Pf + fx + 1];
+        if (cy && cx) {
+            for_cells(l, [&](int jy, int jx, int J) {
+                if (iv[J] == T(0)) return;
+                // fine cells 2J-1 .. 2J+1; the +1 row / column exists only inside the fine box (beyond it the
+                // padded box ends: P gives it no weight and it is not read)
+                const int c = (2 * jy + 1) * Pf + 2 * jx + 1;
+                T s = tf[c] + T(0.5) * (tf[c - 1] + tf[c - Pf]) + T(0.25) * tf[c - Pf - 1];
+                const bool yin = 2 * jy + 1 < hf, xin = 2 * jx + 1 < wf;
+                if (xin) s += T(0.5) * tf[c + 1] + T(0.25) * tf[c - Pf + 1];
+                if (yin) s += T(0.5) * tf[c + Pf] + T(0.25) * tf[c + Pf - 1];
+                if (xin && yin) s += T(0.25) * tf[c + Pf + 1];
+                b[J] = s;
+            });
+        } else {
+            for_cells(l, [&](int jy, int jx, int J) {
+                if (iv[J] == T(0)) return;
+                T s = T(0);
+                for (int ay = (cy ? -1 : 0); ay <= (cy ? 1 : 0); ++ay) {
+                    const int fy = cy ? 2 * jy + ay : jy;
+                    if (fy < 0 || fy >= hf) continue;
+                    const T wa = ay == 0 ? T(1) : T(0.5);
+                    for (int ax = (cx ? -1 : 0); ax <= (cx ? 1 : 0); ++ax) {
+                        const int fx = cx ? 2 * jx + ax : jx;
+                        if (fx < 0 || fx >= wf) continue;
+                        s += wa * (ax == 0 ? T(1) : T(0.5)) * tf[(fy + 1) * Pf + fx + 1];
+                    }
                 }
-            }
-            b[J] = s;
+                b[J] = s;
+            });
         }
         __syncthreads();
     }
 
     // x_l += P x_{l+1} on the active cells of level l.
-    __device__ void prolong_add(int l, T *x, const T *xc) {
-        const int hf = lvh[l], wf = lvw[l], Pf = wf + 2, NPf = (hf + 2) * Pf;
+    __device__ __forceinline__ void prolong_add(int l, T *x, const T *xc) {
+        const int hf = lvh[l], wf = lvw[l], Pf = wf + 2;
         const int hc = lvh[l + 1], wc = lvw[l + 1], Pc = wc + 2;
         const bool cy = hc != hf, cx = wc != wf;
-        auto one = [&](int i) {
-            const int py = i / Pf, fy = py - 1, fx = i - py * Pf - 1;
+        auto one = [&](int fy, int fx, int i) {
             int y0, y1, x0, x1;
             T wy0, wy1, wx0, wx1;
             if (cy) {
@@ -684,26 +838,31 @@ struct Win {
         };
         if (l == 0) {
             const uint16_t *ul = A<uint16_t>(AR_ULIST);
-            for (int k = threadIdx.x; k < nu; k += NT) one(ul[k]);
+            for (int k = threadIdx.x; k < nu; k += NT) {
+                const int i = ul[k];
+                const int py = row0(i);
+                one(py - 1, i - py * Pf - 1, i);
+            }
         } else {
             const T *iv = LV<T>(l, LV_INVD);
-            for (int i = threadIdx.x; i < NPf; i += NT)
-                if (iv[i] != T(0)) one(i);
+            for_cells(l, [&](int fy, int fx, int i) {
+                if (iv[i] != T(0)) one(fy, fx, i);
+            });
         }
     }
 
-    // x = M^+ b on the coarsest level l (its cells in row-major order).
-    __device__ void coarse_solve(int l, const T *b, T *x) {
+    // x = M^+ b on the coarsest level l (its cells in row-major order, padded indices in cidx).
+    __device__ __forceinline__ void coarse_solve(int l, const T *b, T *x) {
         const double *M = A<double>(AR_DENSE);
-        const int hc = lvh[l], wc = lvw[l], Pc = wc + 2, n = hc * wc;
+        const int n = lvh[l] * lvw[l];
         if (threadIdx.x < n) {
             const int u = threadIdx.x;
             double s = 0.0;
             for (int v = 0; v < n; ++v) {
                 const double m = v >= u ? M[u * kNcMax + v] : M[v * kNcMax + u];
-                s += m * static_cast<double>(b[(v / wc + 1) * Pc + v % wc + 1]);
+                s += m * static_cast<double>(b[cidx[v]]);
             }
-            const int iu = (u / wc + 1) * Pc + u % wc + 1;
+            const int iu = cidx[u];
             if (l == 0) {
                 if (A<uint8_t>(AR_MASK)[iu] & M_UNKNOWN) x[iu] = static_cast<T>(s);
             } else {
@@ -716,14 +875,16 @@ struct Win {
     // Solves A d = r0 (r holds r0 on entry, the residual on exit) to relative
     // residual rtol or for at most maxit iterations.  d must be 0 on entry.
     // Returns the iterations; *ok = false on breakdown.
-    __device__ int pcg(T *d, T *r, double rtol, int maxit, bool use_mg, bool *ok) {
+    __device__ __forceinline__ int pcg(T *d, T *r, double rtol, int maxit, bool use_mg, bool *ok) {
         const uint16_t *ul = A<uint16_t>(AR_ULIST);
         const T *gT = A<T>(AR_GT), *invd = A<T>(AR_INVD);
         T *p = A<T>(AR_P), *q = A<T>(AR_Q);
         *ok = true;
         double rz = 0.0, rr = 0.0;
+        mark(PH_RESID);
         if (MG && use_mg) {
             vcycle(r);
+            mark(PH_VCYCLE);
             for (int k = threadIdx.x; k < nu; k += NT) {
                 const int i = ul[k];
                 const T zi = q[i];
@@ -766,8 +927,9 @@ struct Win {
                     d[i] += alpha * p[i];
                     r[i] -= alpha * q[i];
                 }
-                __syncthreads();
+                mark(PH_CG);
                 vcycle(r);
+                mark(PH_VCYCLE);
                 for (int k = threadIdx.x; k < nu; k += NT) {
                     const int i = ul[k];
                     rz2 += static_cast<double>(r[i]) * static_cast<double>(q[i]);
@@ -804,12 +966,13 @@ struct Win {
             }
             __syncthreads();
         }
+        mark(PH_CG);
         return it;
     }
 
     // r = b - A x in FP64 over the unknowns (exact weights up to the
     // reciprocal of 2 sqrt 2), stored as T in AR_R; returns (||r||^2, ||b||^2).
-    __device__ void residual64(double *rr_out, double *bb_out, bool first) {
+    __device__ __forceinline__ void residual64(double *rr_out, double *bb_out, bool first) {
         const uint8_t *mask = A<uint8_t>(AR_MASK);
         const uint16_t *ul = A<uint16_t>(AR_ULIST);
         const double *g64 = A<double>(AR_G64), *x64 = A<double>(AR_X64), *b64 = A<double>(AR_B64);
@@ -847,11 +1010,13 @@ struct Win {
     }
 
     // ---- the solve ----------------------------------------------------------
-    __device__ void solve(WinStat *st) {
+    __device__ __forceinline__ void solve(WinStat *st) {
         const uint16_t *ul = A<uint16_t>(AR_ULIST);
         double *x64 = A<double>(AR_X64);
         const bool want_mg = MG && a.sp.pc == 2;
+        mark(PH_ASSEMBLE);
         if (MG && want_mg) mg_setup();
+        mark(PH_MG_SETUP);
         int iters = 0, outer = 0, status = 1;
         double rel = 0.0;
         if (!REFINE) {
@@ -929,7 +1094,8 @@ struct Win {
     // ---- 5. node currents (grid.cpp:19-71), correction, output --------------
     // out: h x w doubles (pitch w); corr: W x W factors or null, (cy0, cx0) its
     // slice origin.
-    __device__ void currents(double *out, const double *corr, int cy0, int cx0) {
+    __device__ __forceinline__ void currents(double *out, const double *corr, int cy0, int cx0) {
+        mark(PH_RESID);
         const uint8_t *mask = A<uint8_t>(AR_MASK);
         const double *g64 = A<double>(AR_G64), *v = A<double>(AR_X64);
         const bool series = a.series;
@@ -972,6 +1138,7 @@ struct Win {
             out[y * G.w + x] = c;
         }
         __syncthreads();
+        mark(PH_CURRENTS);
     }
 };
 

@@ -277,13 +277,16 @@ def make_params(radius, buffer=0, block_size=1, four_neighbors=False, resistance
     return p
 
 
-def run_device(r, s, params: N.Params, *, normalized=False, out=None):
+def run_device(r, s, params: N.Params, *, normalized=False, out=None, want_stats=True, time_windows=False):
     """One call of ``lsb_omniscape`` on device tensors (float64, contiguous, same device).
 
     Returns ``(outputs, stats)``: outputs is a dict of device tensors ``current``
     and, with the flow potential, ``flow_potential`` (and ``normalized``).  The
     work runs on a side stream ordered after the caller's current stream; the
-    caller's stream waits for it.
+    caller's stream waits for it.  ``want_stats=False`` returns without waiting
+    (stats is then None and device-side solver failures are not reported);
+    ``time_windows=True`` (calls without a graph) also returns the device time
+    of the window kernels in seconds.
     """
     import torch
     lib = N.load()
@@ -306,16 +309,63 @@ def run_device(r, s, params: N.Params, *, normalized=False, out=None):
                 out["flow_potential"] = torch.empty_like(out["current"])
             if normalized:
                 out["normalized"] = torch.empty_like(out["current"])
-        stats = N.Stats()
+        stats = N.Stats() if (want_stats or time_windows) else None
         cur = torch.cuda.current_stream(r.device)
         st.stream.wait_stream(cur)
-        rc = lib.lsb_omniscape(r.data_ptr(), s.data_ptr(), nx, ny, C.byref(params), out["current"].data_ptr(),
-                               out["flow_potential"].data_ptr() if "flow_potential" in out else None,
-                               out["normalized"].data_ptr() if "normalized" in out else None, ws.data_ptr(),
-                               ws.numel(), C.byref(stats), err, len(err), st.stream.cuda_stream)
+        if time_windows:
+            lib.lsb_time_window_kernels(1)
+        try:
+            rc = lib.lsb_omniscape(r.data_ptr(), s.data_ptr(), nx, ny, C.byref(params), out["current"].data_ptr(),
+                                   out["flow_potential"].data_ptr() if "flow_potential" in out else None,
+                                   out["normalized"].data_ptr() if "normalized" in out else None, ws.data_ptr(),
+                                   ws.numel(), C.byref(stats) if stats is not None else None, err, len(err),
+                                   st.stream.cuda_stream)
+        finally:
+            if time_windows:
+                lib.lsb_time_window_kernels(0)
         cur.wait_stream(st.stream)
         N.check(rc, err)
+        if time_windows:
+            return out, stats, stats.window_ms / 1e3
         return out, stats
+
+
+def last_launch_count() -> int:
+    """Kernels the last call on this thread launched (a graph replay: the graph's kernel nodes)."""
+    return int(N.load().lsb_last_launch_count())
+
+
+def window_cells(shape, kw) -> int:
+    """Sum over the targets of a run of the cells of their window boxes; ``kw['active']`` (lattice mask, x outer,
+    y inner) selects the targets, else every block centre counts."""
+    ny, nx = shape
+    D = kw["radius"] + kw.get("buffer", 0)
+    bs = kw.get("block_size", 1)
+    br = (bs - 1) // 2
+    xs = np.arange(br, nx - br, bs)
+    ys = np.arange(br, ny - br, bs)
+    active = kw.get("active")
+    hx = np.minimum(xs + D, nx - 1) - np.maximum(xs - D, 0) + 1
+    hy = np.minimum(ys + D, ny - 1) - np.maximum(ys - D, 0) + 1
+    cells = np.outer(hx, hy)  # lattice order: x outer, y inner
+    if active is not None:
+        cells = cells * active
+    return int(cells.sum())
+
+
+def active_blocks(source, block_size) -> np.ndarray:
+    """Lattice mask (x outer, y inner) of the blocks whose source sum is > 0 (NaN counted as 0)."""
+    s = np.nan_to_num(np.asarray(source, dtype=np.float64), nan=0.0)
+    ny, nx = s.shape
+    bs = int(block_size)
+    br = (bs - 1) // 2
+    nbx = (nx - 2 * br - 1) // bs + 1 if nx - 2 * br > 0 else 0
+    nby = (ny - 2 * br - 1) // bs + 1 if ny - 2 * br > 0 else 0
+    sums = np.zeros((nbx, nby))
+    for dx in range(-br, br + 1):
+        for dy in range(-br, br + 1):
+            sums += s[br + dy: br + dy + bs * nby: bs, br + dx: br + dx + bs * nbx: bs][:nby, :nbx].T
+    return sums > 0
 
 
 def omniscape_correction(radius, buffer, block_size, four_neighbors=False, nx=1000, ny=1000, *,
