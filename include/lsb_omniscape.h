@@ -124,6 +124,28 @@ int lsb_omniscape(const double *resistance, const double *source, int64_t nx, in
                   void *workspace, size_t workspace_bytes, lsb_omni_stats *stats, char *err, size_t errlen,
                   void *stream);
 
+/* Bytes of the static device scratch of lsb_omniscape_noalloc (32 MiB). */
+#define LSB_NOALLOC_SCRATCH_BYTES (32u << 20)
+
+/*
+ * lsb_omniscape without a workspace (no counterpart in the reference).  For
+ * callers that cannot call cudaMalloc -- for instance a host whose device
+ * memory is already reserved by another framework's pool, or code that must
+ * not pay an allocation's implicit device synchronization.  Inputs and outputs
+ * are the caller's device pointers, as for lsb_omniscape; the scratch is one
+ * static device array of LSB_NOALLOC_SCRATCH_BYTES that the library holds on
+ * every GPU where it is loaded, until the process exits.  Window buffers are
+ * streamed in batches sized to fit it; a raster whose targets alone need more
+ * is rejected with LSB_ERR_WORKSPACE and a message.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress); make it
+ * before any stream capture.  Every call shares the array: calls that overlap
+ * on the GPU (other streams, other host threads) race and must be serialised
+ * by the caller.  Launches directly (no graph); allocates nothing.
+ */
+int lsb_omniscape_noalloc(const double *resistance, const double *source, int64_t nx, int64_t ny,
+                          const lsb_omni_params *p, double *current, double *flow_potential, double *normalized,
+                          lsb_omni_stats *stats, char *err, size_t errlen, void *stream);
+
 /* The (2 (radius + buffer) + 1)^2 block-artifact correction factors
  * (omniscape_correction), written to the device array corr. */
 int lsb_omniscape_correction(int32_t radius, int32_t buffer, int32_t block_size, int32_t four_neighbors,

@@ -20,7 +20,7 @@ EDGE_AVERAGE, EDGE_SERIES = 0, 1
 # Every symbol the header declares (the CPU test checks the library exports them).
 EXPORTS = ("lsb_params_default", "lsb_omniscape_workspace_size", "lsb_omniscape", "lsb_omniscape_correction",
            "lsb_omniscape_grad", "lsb_omniscape_grad_workspace_size", "lsb_last_launch_count",
-           "lsb_time_window_kernels", "lsb_version")
+           "lsb_time_window_kernels", "lsb_version", "lsb_omniscape_noalloc")
 
 
 class Condition(C.Structure):
@@ -88,6 +88,9 @@ def load():
         lib.lsb_last_launch_count.restype = i64
         lib.lsb_time_window_kernels.argtypes = [C.c_int32]
         lib.lsb_time_window_kernels.restype = None
+        lib.lsb_omniscape_noalloc.argtypes = [vp, vp, i64, i64, C.POINTER(Params), vp, vp, vp, C.POINTER(Stats),
+                                              C.c_char_p, sz, vp]
+        lib.lsb_omniscape_noalloc.restype = C.c_int
         lib.lsb_version.argtypes = []
         lib.lsb_version.restype = C.c_char_p
         _lib = lib

@@ -612,6 +612,84 @@ int lsb_omniscape(const double *resistance, const double *source, int64_t nx, in
     return LSB_OK;
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// The entry point that allocates nothing.  Its scratch is this file-scope
+// device array: every GPU on which the library is loaded holds it until the
+// process exits.  In host code the name below is only a stand-in for the
+// array; the device address comes from cudaGetSymbolAddress, once per device.
+// ---------------------------------------------------------------------------
+namespace {
+static __device__ __align__(256) unsigned char g_noalloc_scratch[LSB_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void *g_noalloc_ptr[kMaxDevices] = {};
+
+// The device address of the static scratch on the current device (set up on the first call there).
+int noalloc_scratch(void **out, char *err, size_t errlen) {
+    int dev = 0;
+    LSB_CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) {
+        set_err(err, errlen, "device index %d out of range", dev);
+        return LSB_ERR_ARGUMENT;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void *ptr = nullptr;
+        LSB_CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+        g_noalloc_ptr[dev] = ptr;
+    }
+    *out = g_noalloc_ptr[dev];
+    return LSB_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int lsb_omniscape_noalloc(const double *resistance, const double *source, int64_t nx, int64_t ny,
+                          const lsb_omni_params *p, double *current, double *flow_potential, double *normalized,
+                          lsb_omni_stats *stats, char *err, size_t errlen, void *stream) {
+    if (!p) {
+        set_err(err, errlen, "params is NULL");
+        return LSB_ERR_ARGUMENT;
+    }
+    // the same call as lsb_omniscape, launched directly (no graph), with the window buffers of a batch sized
+    // so that the whole workspace fits the static array
+    lsb_omni_params q = *p;
+    q.use_graph = 0;
+    const size_t cap = LSB_NOALLOC_SCRATCH_BYTES;
+    Plan pl;
+    int rc = make_plan(nx, ny, &q, &pl, err, errlen);
+    if (rc) return rc;
+    if (pl.total > cap) {
+        const size_t per_window = static_cast<size_t>(pl.g.W) * pl.g.W * 8 * (pl.g.fp ? 2 : 1);
+        const size_t windows = static_cast<size_t>(pl.batch) * per_window;
+        const size_t fixed = pl.total - std::min(pl.total, windows);
+        int64_t batch = fixed + 4 * kAlign < cap ? static_cast<int64_t>((cap - fixed - 4 * kAlign) / per_window) : 0;
+        while (batch >= 1) {
+            q.memory_limit = static_cast<double>(batch) * static_cast<double>(per_window);
+            rc = make_plan(nx, ny, &q, &pl, err, errlen);
+            if (rc) return rc;
+            if (pl.total <= cap) break;
+            batch = batch * 9 / 10;
+        }
+        if (batch < 1 || pl.total > cap) {
+            set_err(err, errlen,
+                    "lsb_omniscape_noalloc: this raster and window size need more than the %zu bytes of static "
+                    "scratch (at least %zu); call lsb_omniscape with a workspace instead",
+                    cap, fixed + per_window);
+            return LSB_ERR_WORKSPACE;
+        }
+    }
+    void *ws = nullptr;
+    rc = noalloc_scratch(&ws, err, errlen);
+    if (rc) return rc;
+    return lsb_omniscape(resistance, source, nx, ny, &q, current, flow_potential, normalized, ws, cap, stats, err,
+                         errlen, stream);
+}
+
 int lsb_omniscape_correction(int32_t radius, int32_t buffer, int32_t block_size, int32_t four_neighbors,
                              int32_t edge_weights, int64_t nx, int64_t ny, double *corr, void *workspace,
                              size_t workspace_bytes, char *err, size_t errlen, void *stream) {
