@@ -288,7 +288,7 @@ int make_plan(int64_t nx, int64_t ny, const lsb_omni_params *p, Plan *pl, char *
     pl->o_fp = take(g.fp ? static_cast<size_t>(batch) * g.W * g.W * 8 : 0);
     pl->o_gs = take(static_cast<size_t>(pl->grid) * pl->lay.gmem_bytes);
     pl->o_devstats = take(sizeof(DevStats));
-    pl->o_timers = take(sizeof(unsigned long long) * 32);
+    pl->o_timers = take(sizeof(unsigned long long) * 32);  // >= PH_COUNT
     pl->total = o;
     return LSB_OK;
 }
@@ -298,7 +298,7 @@ SolveParams solve_params(const lsb_omni_params *p) {
     sp.tol = p->tol > 0 ? p->tol : 1e-12;
     sp.inner_tol = p->precision == LSB_PREC_FP64 ? sp.tol : 1e-4;
     sp.max_iter = p->max_iter > 0 ? p->max_iter : 20000;
-    sp.max_outer = 30;
+    sp.max_outer = 12;
     sp.pc = resolved_pc(p);
     sp.omega = 0.7f;
     return sp;
@@ -388,7 +388,7 @@ int enqueue(const Plan &pl, const double *res, const double *src, const lsb_omni
     a.lay = pl.lay;
 #ifdef LSB_PHASE_TIMERS
     a.timers = reinterpret_cast<unsigned long long *>(ws + pl.o_timers);
-    LSB_CK(cudaMemsetAsync(a.timers, 0, sizeof(unsigned long long) * 32, s));
+    LSB_CK(cudaMemsetAsync(a.timers, 0, sizeof(unsigned long long) * 30, s));
 #endif
     a.sp = solve_params(p);
     if (g.conditions && g.NL > 0) {
@@ -409,7 +409,6 @@ int enqueue(const Plan &pl, const double *res, const double *src, const lsb_omni
         c.stat = reinterpret_cast<WinStat *>(ws + pl.o_corrstat);
         c.queue = queue + pl.nbatches;
         c.correct = 0;
-        c.sp.tol = std::min(c.sp.tol, 1e-13);
         pl.kern<<<2, pl.v.nt, pl.lay.smem_bytes, s>>>(c);
         k_corr_ratio<<<1, 1024, 0, s>>>(c.cur_win, c.stat, g.W, g.bs, reinterpret_cast<double *>(ws + pl.o_corr));
         launches += 2;
@@ -578,15 +577,19 @@ int lsb_omniscape(const double *resistance, const double *source, int64_t nx, in
         {
             unsigned long long tm[PH_COUNT];
             LSB_CK(cudaMemcpy(tm, ws + pl.o_timers, sizeof tm, cudaMemcpyDeviceToHost));
-            static const char *names[PH_COUNT] = {"load", "flood", "mark", "assemble", "mg_setup", "resid64",
-                                                  "cg", "vcycle", "currents", "other"};
+            static const char *names[PH_COUNT] = {"load", "flood", "mark", "assemble", "mg_setup", "resid64", "cg",
+                                                  "vcycle", "currents", "other", "v_pre0", "v_restrict1", "v_down",
+                                                  "v_coarsest", "v_up", "v_prolong0", "v_post0"};
             double tot = 0;
             for (int k = 0; k < PH_COUNT; ++k) tot += static_cast<double>(tm[k]);
             fprintf(stderr, "[phases] windows=%d cycles/window:", hdr[0]);
             for (int k = 0; k < PH_COUNT; ++k)
                 fprintf(stderr, " %s=%.0f(%.0f%%)", names[k], tm[k] / std::max(1.0, static_cast<double>(hdr[0])),
                         100.0 * tm[k] / std::max(tot, 1.0));
-            fprintf(stderr, "\n");
+            unsigned long long cal[2];
+            LSB_CK(cudaMemcpy(cal, ws + pl.o_timers + 30 * sizeof(unsigned long long), sizeof cal,
+                              cudaMemcpyDeviceToHost));
+            fprintf(stderr, " | barrier=%llu cycles, barrier+smem round trip=%llu cycles\n", cal[0], cal[1]);
         }
 #endif
         stats->n_targets = hdr[0];
@@ -744,7 +747,6 @@ int lsb_omniscape_correction(int32_t radius, int32_t buffer, int32_t block_size,
     c.gscratch = reinterpret_cast<char *>(queue) + align_up(8);
     c.lay = pl.lay;
     c.sp = solve_params(&p);
-    c.sp.tol = 1e-13;
     LSB_CK(cudaMemsetAsync(queue, 0, 4, s));
     pl.kern<<<2, pl.v.nt, pl.lay.smem_bytes, s>>>(c);
     k_corr_ratio<<<1, 1024, 0, s>>>(c.cur_win, c.stat, g.W, g.bs, corr);

@@ -59,11 +59,13 @@ struct Nb<true> {
     __host__ __device__ static constexpr bool diag(int) { return false; }
 };
 
-// Exact edge weight of two conductances (grid.hpp:37-40; resistor series:
-// circuitscape.cpp:30-33), used where the reference's rounding matters.
-__device__ __forceinline__ double edge_w_exact(double a, double b, bool diag, bool series) {
+// FP64 edge weight of two conductances (grid.hpp:37-40; resistor series:
+// circuitscape.cpp:30-33).  The diagonal average multiplies by 1 / (2 sqrt 2)
+// where the reference divides by 2 sqrt 2: within one ulp of the reference's
+// weight, far below the solver's tolerance.
+__device__ __forceinline__ double edge_w64(double a, double b, bool diag, bool series) {
     if (series) return diag ? 1.0 / (kSqrt2 * (1.0 / a + 1.0 / b) / 2.0) : 1.0 / ((1.0 / a + 1.0 / b) / 2.0);
-    return diag ? (a + b) / kTwoSqrt2 : (a + b) / 2.0;
+    return diag ? (a + b) * kInvTwoSqrt2 : (a + b) * 0.5;
 }
 
 // ---------------------------------------------------------------------------

@@ -29,6 +29,23 @@ __global__ void __launch_bounds__(NT, 1) k_windows(const KArgs a) {
     if (threadIdx.x <= PH_COUNT) tacc[threadIdx.x] = threadIdx.x == PH_COUNT ? clock64() : 0ull;
     __syncthreads();
     win.tacc = tacc;
+    if (blockIdx.x == 0 && a.timers) {
+        // calibration: 64 bare barriers, then 64 barrier-separated shared-memory round trips
+        __shared__ float cal[1024];
+        unsigned long long t0 = clock64();
+        for (int k = 0; k < 64; ++k) __syncthreads();
+        unsigned long long t1 = clock64();
+        for (int k = 0; k < 64; ++k) {
+            cal[threadIdx.x] = cal[(threadIdx.x + 1) % NT] + 1.0f;
+            __syncthreads();
+        }
+        unsigned long long t2 = clock64();
+        if (threadIdx.x == 0) {
+            a.timers[30] = (t1 - t0) / 64;
+            a.timers[31] = (t2 - t1) / 64;
+        }
+        __syncthreads();
+    }
 #endif
     int count;
     if (a.mode == 1) {
