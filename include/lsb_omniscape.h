@@ -155,8 +155,10 @@ int lsb_omniscape_correction(int32_t radius, int32_t buffer, int32_t block_size,
 /*
  * Adjoint of the cumulative current.  J = sum over cells of weight * current;
  * writes dJ/d(resistance) (dJ/d(conductance) with resistance_is_conductance)
- * to grad_resistance and dJ/d(source) to grad_source (either may be NULL),
- * and J to *J_out when J_out != NULL (device pointer to one double).
+ * to grad_resistance (required) and dJ/d(source) to grad_source (NULL: not
+ * written), and J to *J_out when J_out != NULL (device pointer to one double).
+ * weight is a device ny x nx raster; backward through J = sum(weight * current)
+ * is the vector-Jacobian product of the cumulative current.
  * Forward potentials are recomputed, not stored; each window's adjoint
  * system is the same symmetric Laplacian with the node-current derivative as
  * right-hand side.  Needs no correction (block_size 1 or correct_artifacts 0)

@@ -16,4 +16,6 @@ from .omni import (  # noqa: F401
     source_from_resistance,
 )
 
+from .autograd import grad_device, omniscape_current  # noqa: F401,E402
+
 __version__ = "0.1.0"

@@ -146,7 +146,7 @@ int resolved_pc(const lsb_omni_params *p) {
 
 constexpr size_t kStaticSmem = 2048;  // the window kernel's static shared memory, with room to spare
 
-ArenaLayout make_layout(const Variant &v, int W, size_t smem_budget) {
+ArenaLayout make_layout(const Variant &v, int W, size_t smem_budget, bool grad) {
     ArenaLayout L;
     std::memset(&L, 0, sizeof L);
     const size_t np = static_cast<size_t>(W + 2) * (W + 2);
@@ -181,6 +181,11 @@ ArenaLayout make_layout(const Variant &v, int W, size_t smem_budget) {
     if (has_d) items.push_back({AR_X64, np * 8});
     items.push_back({AR_G64, np * 8});
     items.push_back({AR_B64, np * 8});
+    if (grad) {
+        items.push_back({AR_V64, np * 8});
+        items.push_back({AR_CW, np * 8});
+        items.push_back({AR_DG64, np * 8});
+    }
     size_t so = 0, go = 0;
     for (const Item &it : items) {
         const size_t b = align_up(it.bytes, 16);
@@ -236,18 +241,25 @@ struct Plan {
     int nparts;         // scan blocks
     // workspace offsets
     size_t o_amps, o_tindex, o_targets, o_part, o_count, o_queue, o_err, o_stat, o_condv, o_corr, o_corrwin,
-        o_corrstat, o_cur, o_fp, o_gs, o_devstats, o_timers, total;
+        o_corrstat, o_cur, o_fp, o_gs, o_devstats, o_timers, o_jw, total;
+    bool grad;
 };
 
-int make_plan(int64_t nx, int64_t ny, const lsb_omni_params *p, Plan *pl, char *err, size_t errlen) {
+int make_plan(int64_t nx, int64_t ny, const lsb_omni_params *p, Plan *pl, char *err, size_t errlen,
+              bool grad = false) {
     int rc = make_geom(nx, ny, p, &pl->g, err, errlen);
     if (rc) return rc;
+    pl->grad = grad;
+    if (grad) {
+        // the gradient windows of a batch (resistance, source) use the two window slots
+        pl->g.fp = true;
+    }
     const Geom &g = pl->g;
     pl->v = choose_variant(p, g);
     DeviceInfo di;
     LSB_CK(device_info(&di));
     const size_t budget = di.smem_optin > kStaticSmem ? di.smem_optin - kStaticSmem : 0;
-    pl->lay = make_layout(pl->v, g.W, budget);
+    pl->lay = make_layout(pl->v, g.W, budget, grad);
     pl->kern = pick(pl->v);
     LSB_CK(cudaFuncSetAttribute(reinterpret_cast<const void *>(pl->kern),
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(pl->lay.smem_bytes)));
@@ -289,6 +301,7 @@ int make_plan(int64_t nx, int64_t ny, const lsb_omni_params *p, Plan *pl, char *
     pl->o_gs = take(static_cast<size_t>(pl->grid) * pl->lay.gmem_bytes);
     pl->o_devstats = take(sizeof(DevStats));
     pl->o_timers = take(sizeof(unsigned long long) * 32);  // >= PH_COUNT
+    pl->o_jw = take(grad ? NL * 8 : 0);
     pl->total = o;
     return LSB_OK;
 }
@@ -756,14 +769,144 @@ int lsb_omniscape_correction(int32_t radius, int32_t buffer, int32_t block_size,
 }
 
 int lsb_omniscape_grad_workspace_size(int64_t nx, int64_t ny, const lsb_omni_params *p, size_t *bytes) {
-    return lsb_omniscape_workspace_size(nx, ny, p, bytes);
+    Plan pl;
+    const int rc = make_plan(nx, ny, p, &pl, nullptr, 0, true);
+    if (rc) return rc;
+    *bytes = pl.total;
+    return LSB_OK;
 }
 
-int lsb_omniscape_grad(const double *, const double *, const double *, int64_t, int64_t, const lsb_omni_params *,
-                       double *, double *, double *, void *, size_t, lsb_omni_stats *, char *err, size_t errlen,
-                       void *) {
-    set_err(err, errlen, "the adjoint is not built in this version");
-    return LSB_ERR_ARGUMENT;
+int lsb_omniscape_grad(const double *resistance, const double *source, const double *weight, int64_t nx, int64_t ny,
+                       const lsb_omni_params *p, double *grad_resistance, double *grad_source, double *J_out,
+                       void *workspace, size_t workspace_bytes, lsb_omni_stats *stats, char *err, size_t errlen,
+                       void *stream) {
+    if (!p) {
+        set_err(err, errlen, "params is NULL");
+        return LSB_ERR_ARGUMENT;
+    }
+    if (p->correct_artifacts && p->block_size > 1) {
+        set_err(err, errlen, "the adjoint needs no block-artifact correction (block_size 1 or correct_artifacts 0)");
+        return LSB_ERR_ARGUMENT;
+    }
+    if (p->condition1.present || p->condition2.present) {
+        set_err(err, errlen, "the adjoint does not support conditions");
+        return LSB_ERR_ARGUMENT;
+    }
+    Plan pl;
+    int rc = make_plan(nx, ny, p, &pl, err, errlen, true);
+    if (rc) return rc;
+    if (!resistance || !source || !weight || !grad_resistance) {
+        set_err(err, errlen, "resistance, source, weight and grad_resistance are required");
+        return LSB_ERR_ARGUMENT;
+    }
+    if (!workspace || workspace_bytes < pl.total) {
+        set_err(err, errlen, "workspace too small: %zu bytes needed", pl.total);
+        return LSB_ERR_WORKSPACE;
+    }
+    const Geom &g = pl.g;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    char *ws = static_cast<char *>(workspace);
+    const int64_t n = g.nx * g.ny;
+    int64_t launches = 0;
+    LSB_CK(cudaMemsetAsync(grad_resistance, 0, n * 8, s));
+    if (grad_source) LSB_CK(cudaMemsetAsync(grad_source, 0, n * 8, s));
+    LSB_CK(cudaMemsetAsync(ws + pl.o_count, 0, 4, s));
+    LSB_CK(cudaMemsetAsync(ws + pl.o_queue, 0, (pl.nbatches + 1) * 4, s));
+    LSB_CK(cudaMemsetAsync(ws + pl.o_err, 0, 4, s));
+    double *amps = reinterpret_cast<double *>(ws + pl.o_amps);
+    int *tindex = reinterpret_cast<int *>(ws + pl.o_tindex), *targets = reinterpret_cast<int *>(ws + pl.o_targets);
+    int *part = reinterpret_cast<int *>(ws + pl.o_part), *count = reinterpret_cast<int *>(ws + pl.o_count);
+    int *queue = reinterpret_cast<int *>(ws + pl.o_queue);
+    WinStat *stat = reinterpret_cast<WinStat *>(ws + pl.o_stat);
+    double *Jw = reinterpret_cast<double *>(ws + pl.o_jw);
+    LSB_CK(cudaMemsetAsync(stat, 0, std::max<int64_t>(g.NL, 1) * 2 * sizeof(WinStat), s));
+    if (g.NL > 0) {
+        const int nb = static_cast<int>((g.NL + 255) / 256);
+        k_lattice_amps<<<nb, 256, 0, s>>>(source, g.nx, g.ny, g.bs, g.br, g.nbx, g.nby, amps);
+        k_scan_count<<<pl.nparts, kScanBlock, 0, s>>>(amps, g.NL, part);
+        k_scan_offsets<<<1, 1024, 0, s>>>(part, pl.nparts, count);
+        k_scan_write<<<pl.nparts, kScanBlock, 0, s>>>(amps, g.NL, part, tindex, targets);
+        launches += 4;
+        LSB_CK(cudaGetLastError());
+    }
+    KArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.res = resistance;
+    a.src = source;
+    a.nx = g.nx;
+    a.ny = g.ny;
+    a.R = g.R;
+    a.D = g.D;
+    a.W = g.W;
+    a.bs = g.bs;
+    a.br = g.br;
+    a.nbx = g.nbx;
+    a.nby = g.nby;
+    a.ric = p->resistance_is_conductance != 0;
+    a.series = p->edge_weights == LSB_EDGE_SERIES;
+    a.four = p->four_neighbors != 0;
+    a.fp = 0;
+    a.correct = 0;
+    a.count_ptr = count;
+    a.targets = targets;
+    a.lat_amps = amps;
+    a.gscratch = ws + pl.o_gs;
+    a.lay = pl.lay;
+    a.sp = solve_params(p);
+    a.mode = 2;
+    a.weight = weight;
+    a.Jw = Jw;
+    a.cur_win = reinterpret_cast<double *>(ws + pl.o_cur);
+    a.fp_win = reinterpret_cast<double *>(ws + pl.o_fp);
+    a.stat = stat;
+    a.batch_size = static_cast<int>(pl.batch);
+    const dim3 gg(static_cast<unsigned>((g.nx + kGatherTX - 1) / kGatherTX),
+                  static_cast<unsigned>((g.ny + kGatherTY - 1) / kGatherTY));
+    for (int b = 0; b < pl.nbatches && g.NL > 0; ++b) {
+        a.batch_start = static_cast<int>(b * pl.batch);
+        a.queue = queue + b;
+        pl.kern<<<pl.grid, pl.v.nt, pl.lay.smem_bytes, s>>>(a);
+        k_gather<<<gg, kGatherTX * kGatherTY, 0, s>>>(a, tindex, grad_resistance, grad_source);
+        launches += 2;
+        LSB_CK(cudaGetLastError());
+    }
+    if (J_out) {
+        if (g.NL > 0) {
+            k_sum_targets<<<1, 1024, 0, s>>>(Jw, count, J_out);
+            ++launches;
+        } else {
+            LSB_CK(cudaMemsetAsync(J_out, 0, 8, s));
+        }
+        LSB_CK(cudaGetLastError());
+    }
+    k_stats<<<1, 1024, 0, s>>>(stat, count, 2, reinterpret_cast<DevStats *>(ws + pl.o_devstats));
+    ++launches;
+    LSB_CK(cudaGetLastError());
+    g_launches = launches;
+    if (stats) {
+        DevStats ds;
+        int cnt = 0;
+        LSB_CK(cudaMemcpyAsync(&ds, ws + pl.o_devstats, sizeof ds, cudaMemcpyDeviceToHost, s));
+        LSB_CK(cudaMemcpyAsync(&cnt, ws + pl.o_count, 4, cudaMemcpyDeviceToHost, s));
+        LSB_CK(cudaStreamSynchronize(s));
+        std::memset(stats, 0, sizeof *stats);
+        stats->n_targets = cnt;
+        stats->n_solved = ds.n_solved;
+        stats->n_failed = ds.n_failed;
+        stats->iters_total = ds.iters_total;
+        stats->iters_max = ds.iters_max;
+        stats->refine_max = ds.refine_max;
+        stats->batches = pl.nbatches;
+        stats->threads_per_window = pl.v.nt;
+        stats->preconditioner = resolved_pc(p);
+        stats->worst_residual = ds.worst_residual;
+        if (ds.n_failed > 0) {
+            set_err(err, errlen, "%lld window solves of the adjoint did not converge (worst relative residual %.3g)",
+                    static_cast<long long>(ds.n_failed), ds.worst_residual);
+            return LSB_ERR_NOT_CONVERGED;
+        }
+    }
+    return LSB_OK;
 }
 
 int64_t lsb_last_launch_count(void) { return g_launches; }

@@ -68,6 +68,16 @@ __device__ __forceinline__ double edge_w64(double a, double b, bool diag, bool s
     return diag ? (a + b) * kInvTwoSqrt2 : (a + b) * 0.5;
 }
 
+// d(edge weight)/d(first conductance); the weights are symmetric in their arguments.
+__device__ __forceinline__ double edge_dw64(double a, double b, bool diag, bool series) {
+    if (series) {
+        // w = 2 / (k (1/a + 1/b)), k = sqrt 2 on diagonals: dw/da = 2 / (k (1/a + 1/b)^2 a^2)
+        const double k = diag ? kSqrt2 : 1.0, s = 1.0 / a + 1.0 / b;
+        return 2.0 / (k * s * s * a * a);
+    }
+    return diag ? kInvTwoSqrt2 : 0.5;
+}
+
 // ---------------------------------------------------------------------------
 // Window descriptions.
 // ---------------------------------------------------------------------------
@@ -82,7 +92,7 @@ struct WinGeom {
 };
 
 // Mask bits of a level-0 cell.
-enum : uint8_t { M_UNKNOWN = 1, M_PRESENT = 2, M_CAND = 4 };
+enum : uint8_t { M_UNKNOWN = 1, M_PRESENT = 2, M_CAND = 4, M_USEIN = 8 };
 
 constexpr int kMaxLevels = 9;  // level 0 + up to 8 coarse levels (windows up to 513 cells wide)
 constexpr int kNcMax = 25;     // cells of the coarsest level (solved by its dense inverse)
@@ -95,6 +105,9 @@ enum ArenaArray : int {
     AR_G64,       // f64: conductance (-9999 outside / NoData; 0 on padding)
     AR_X64,       // f64: solution (potentials), 0 off the unknowns
     AR_B64,       // f64: scaled sources (the right-hand side)
+    AR_V64,       // f64: the forward potentials, kept during the adjoint solve
+    AR_CW,        // f64: J's weight of each cell (adjoint)
+    AR_DG64,      // f64: the explicit part of dJ/dg (adjoint)
     AR_GT,        // T: stencil conductance (or resistance with series weights); sentinels off the nodes
     AR_INVD,      // T: 1 / diagonal on the unknowns, 0 elsewhere
     AR_D,         // T: inner solution (refinement correction)

@@ -285,6 +285,18 @@ __global__ void k_finish(const double *__restrict__ res, int64_t n, double *__re
     }
 }
 
+// Sum of the targets' shares of J (one CTA, fixed order): *out = sum over t < count of Jw[t].
+__global__ void __launch_bounds__(1024) k_sum_targets(const double *__restrict__ Jw, const int *__restrict__ count_ptr,
+                                                      double *__restrict__ out) {
+    __shared__ double red_buf[128];
+    Reducer<1024> red{red_buf, 0};
+    const int n = *count_ptr;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += 1024) s += Jw[i];
+    s = red.sum(s);
+    if (threadIdx.x == 0) *out = s;
+}
+
 // Aggregate statistics (one CTA, fixed order).
 struct DevStats {
     long long n_solved, n_failed, iters_total;

@@ -43,6 +43,7 @@ struct KArgs {
     const double *weight;
     // per-phase cycle counters (builds with LSB_PHASE_TIMERS only)
     unsigned long long *timers;
+    double *Jw;  // mode 2: J's share of every target
 };
 
 // Phases of a window solve, for the cycle counters of profiling builds.
@@ -118,6 +119,7 @@ struct Win {
     WinGeom G;
     int nu = 0;      // number of unknowns
     int nlev = 1;
+    double src_sum = 0.0;  // the landscape window's sum of positive raw sources (the scaling denominator)
 #ifdef LSB_PHASE_TIMERS
     unsigned long long *tacc = nullptr;  // shared, PH_COUNT + 1 (the last: time of the previous mark)
 #endif
@@ -202,6 +204,7 @@ struct Win {
             return 0.0;
         }
         const double sum = red.sum(pos);  // ends with a barrier
+        src_sum = sum;
         // rescale the positive sources to the block's amps (omniscape.cpp:520-525)
         if (kind == KIND_CORR_NULL) {
             const double v = 1.0 / (a.n_corr_sources - 1.0);
@@ -1048,12 +1051,14 @@ struct Win {
     }
 
     // ---- the solve ----------------------------------------------------------
-    __device__ __forceinline__ void solve(WinStat *st) {
+    // x64 must be zero on entry; with setup == false the multigrid hierarchy of the previous solve of the same
+    // matrix is reused.
+    __device__ __forceinline__ void solve(WinStat *st, bool setup = true) {
         const uint16_t *ul = A<uint16_t>(AR_ULIST);
         double *x64 = A<double>(AR_X64);
         const bool want_mg = MG && a.sp.pc == 2;
         mark(PH_ASSEMBLE);
-        if (MG && want_mg) mg_setup();
+        if (MG && want_mg && setup) mg_setup();
         mark(PH_MG_SETUP);
         int iters = 0, outer = 0, status = 1;
         double rel = 0.0;
@@ -1136,6 +1141,161 @@ struct Win {
             st->status = status;
             st->resid = static_cast<float>(rel);
         }
+    }
+
+    // ---- adjoint of J = sum over the window of weight x node current ---------
+    // With b_qm = w_qm (v_m - v_q) the branch current into q from m, the node
+    // current is cur_q = max(in_q, out_q) over the counted branches
+    // (grid.cpp:39-71), so dcur_q/db_qm = s_q(m) in {-1, 0, 1}: +1 for a
+    // counted inflow when the inflow wins, -1 for a counted outflow when the
+    // outflow wins.  With K_nm = W_n s_n(m) - W_m s_m(n):
+    //   dJ/dv_n           = -sum_m w_nm K_nm
+    //   dJ/dg_n (explicit) = sum_m dw_nm/dg_n (v_m - v_n) K_nm
+    //   dJ/dg_n (through A) = -sum_m dw_nm/dg_n (l_n - l_m)(v_n - v_m),  A l = dJ/dv.
+    __device__ __forceinline__ int branch_sel(bool use_in, double b, double maxin, double maxout) const {
+        if (use_in) return (b > 0 && !(fabs(b / maxin) < 1e-8)) ? 1 : 0;
+        return (b < 0 && !(fabs(b / maxout) < 1e-8)) ? -1 : 0;
+    }
+
+    // After the forward solve (x64 = v): J's share of the window, dJ/dv as the right-hand side of the adjoint
+    // solve (B64), the explicit dJ/dg (DG64), v kept in V64, x64 cleared.  *any: the window has a nonzero
+    // J weight on a node.
+    __device__ __forceinline__ double adjoint_prep(bool *any) {
+        uint8_t *mask = A<uint8_t>(AR_MASK);
+        const double *g64 = A<double>(AR_G64);
+        double *v = A<double>(AR_X64), *b64 = A<double>(AR_B64), *v64 = A<double>(AR_V64),
+               *cw = A<double>(AR_CW), *dg = A<double>(AR_DG64);
+        const bool series = a.series;
+        double maxout = -CUDART_INF, maxin = -CUDART_INF;
+        for (int i = threadIdx.x; i < G.NP; i += NT) {
+            if (!(mask[i] & M_PRESENT)) continue;
+            const double gi = g64[i], vi = v[i];
+#pragma unroll
+            for (int dd = LOWER; dd < ND; ++dd) {
+                const int n = i + noff(dd);
+                if (!(mask[n] & M_PRESENT)) continue;
+                const double b = edge_w64(gi, g64[n], NB::diag(dd), series) * (v[n] - vi);
+                if (b > maxout) maxout = b;
+                if (-b > maxin) maxin = -b;
+            }
+        }
+        red.max2(maxout, maxin);
+        double J = 0.0, wabs = 0.0;
+        for (int i = threadIdx.x; i < G.NP; i += NT) {
+            const int py = row0(i), y = py - 1, x = i - py * G.P - 1;
+            double W = 0.0;
+            uint8_t m = mask[i];
+            if (y >= 0 && y < G.h && x >= 0 && x < G.w && (m & M_PRESENT)) {
+                W = a.weight[(G.y0 + y) * a.nx + (G.x0 + x)];
+                const double gi = g64[i], vi = v[i];
+                double inflow = 0.0, outflow = 0.0;
+#pragma unroll
+                for (int dd = 0; dd < ND; ++dd) {
+                    const int n = i + noff(dd);
+                    if (!(mask[n] & M_PRESENT)) continue;
+                    const double b = edge_w64(gi, g64[n], NB::diag(dd), series) * (v[n] - vi);
+                    if (b > 0) {
+                        if (!(fabs(b / maxin) < 1e-8)) inflow += b;
+                    } else if (b < 0) {
+                        if (!(fabs(b / maxout) < 1e-8)) outflow -= b;
+                    }
+                }
+                J += W * (inflow > outflow ? inflow : outflow);
+                wabs += fabs(W);
+                m = inflow > outflow ? (m | M_USEIN) : (m & ~M_USEIN);
+                mask[i] = m;
+            }
+            cw[i] = W;
+        }
+        red.sum2(J, wabs);  // barrier: cw and the M_USEIN bits visible
+        *any = wabs > 0.0;
+        for (int i = threadIdx.x; i < G.NP; i += NT) {
+            const uint8_t mi = mask[i];
+            double dvi = 0.0, dgi = 0.0;
+            if (mi & M_PRESENT) {
+                const double gi = g64[i], vi = v[i], Wi = cw[i];
+                const bool ini = (mi & M_USEIN) != 0;
+#pragma unroll
+                for (int dd = 0; dd < ND; ++dd) {
+                    const int n = i + noff(dd);
+                    const uint8_t mn = mask[n];
+                    if (!(mn & M_PRESENT)) continue;
+                    const double gn = g64[n];
+                    const double we = edge_w64(gi, gn, NB::diag(dd), series);
+                    const double b = we * (v[n] - vi);  // into i from n; from n's side it is -b exactly
+                    const double K = Wi * branch_sel(ini, b, maxin, maxout) -
+                                     cw[n] * branch_sel((mn & M_USEIN) != 0, -b, maxin, maxout);
+                    dvi -= we * K;
+                    dgi += edge_dw64(gi, gn, NB::diag(dd), series) * (v[n] - vi) * K;
+                }
+            }
+            b64[i] = (mi & M_UNKNOWN) ? dvi : 0.0;
+            dg[i] = dgi;
+            v64[i] = v[i];
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < G.NP; i += NT) v[i] = 0.0;
+        __syncthreads();
+        return J;
+    }
+
+    // The window's raw source at (y, x) (within radius, NaN as 0, the target block zeroed as load() does).
+    __device__ __forceinline__ double raw_source(int y, int x) const {
+        const int dy = y - G.gy, dx = x - G.gx, R = a.R, D = a.D, br = a.br;
+        double s = 0.0;
+        if (dy * dy + dx * dx <= R * R) {
+            s = a.src[(G.y0 + y) * a.nx + (G.x0 + x)];
+            if (isnan(s)) s = 0.0;
+        }
+        const int64_t ylim = (D + br < a.ny - 1 ? D + br : a.ny - 1), xlim = (D + br < a.nx - 1 ? D + br : a.nx - 1);
+        if (y >= D - br && y <= ylim && x >= D - br && x <= xlim) s = 0.0;
+        return s;
+    }
+
+    // After the adjoint solve (x64 = l): dJ/d(resistance) of the window to out_r and dJ/d(source) to out_s
+    // (h x w each, pitch w), chained through g = 1/r and the source scaling src = raw amps / sum.
+    __device__ __forceinline__ void grad_finish(double *out_r, double *out_s, double amps) {
+        const uint8_t *mask = A<uint8_t>(AR_MASK);
+        const double *g64 = A<double>(AR_G64), *lam = A<double>(AR_X64), *v64 = A<double>(AR_V64),
+                     *dg = A<double>(AR_DG64);
+        const bool series = a.series;
+        double slam = 0.0;
+        for (int i = threadIdx.x; i < G.NP; i += NT) {
+            const int py = row0(i), y = py - 1, x = i - py * G.P - 1;
+            if (y < 0 || y >= G.h || x < 0 || x >= G.w) continue;
+            const uint8_t mi = mask[i];
+            double dr = 0.0;
+            if (mi & M_PRESENT) {
+                const double gi = g64[i], li = lam[i], vi = v64[i];
+                double dgi = dg[i];
+#pragma unroll
+                for (int dd = 0; dd < ND; ++dd) {
+                    const int n = i + noff(dd);
+                    if (!(mask[n] & M_PRESENT)) continue;
+                    dgi -= edge_dw64(gi, g64[n], NB::diag(dd), series) * (li - lam[n]) * (vi - v64[n]);
+                }
+                const double r = a.res[(G.y0 + y) * a.nx + (G.x0 + x)];
+                dr = a.ric ? dgi : -dgi / (r * r);
+            }
+            out_r[y * G.w + x] = dr;
+            const double raw = raw_source(y, x);
+            if (raw > 0) slam += raw * lam[i];
+        }
+        slam = red.sum(slam);
+        const double sum = src_sum;
+        for (int i = threadIdx.x; i < G.NP; i += NT) {
+            const int py = row0(i), y = py - 1, x = i - py * G.P - 1;
+            if (y < 0 || y >= G.h || x < 0 || x >= G.w) continue;
+            const double raw = raw_source(y, x);
+            double ds = raw > 0 ? (amps / sum) * lam[i] - (amps / (sum * sum)) * slam : 0.0;
+            // amps: the block's sum of sources (NaN skipped) around the target
+            const int64_t my = G.y0 + y, mx = G.x0 + x;
+            if (my >= G.ty - a.br && my <= G.ty + a.br && mx >= G.tx - a.br && mx <= G.tx + a.br &&
+                !isnan(a.src[my * a.nx + mx]))
+                ds += slam / sum;
+            out_s[y * G.w + x] = ds;
+        }
+        __syncthreads();
     }
 
     // ---- 5. node currents (grid.cpp:19-71), correction, output --------------

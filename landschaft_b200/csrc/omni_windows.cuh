@@ -59,6 +59,7 @@ __global__ void __launch_bounds__(NT, 1) k_windows(const KArgs a) {
     // through a single code path, so that the solver is expanded once in the kernel.
     int item = 0, job = 0, njobs = 0;
     int t = 0, L = 0, cy0 = 0, cx0 = 0;
+    bool adj_go = false;  // mode 2: the forward window has a J weight on a node
     while (true) {
         if (job == njobs) {
             if (threadIdx.x == 0) item_s = atomicAdd(a.queue, 1);
@@ -75,7 +76,7 @@ __global__ void __launch_bounds__(NT, 1) k_windows(const KArgs a) {
                 G.y0 = G.x0 = 0;
                 G.ty = G.tx = D;
             } else {
-                njobs = a.fp ? 2 : 1;
+                njobs = (a.fp || a.mode == 2) ? 2 : 1;
                 t = a.batch_start + item;
                 L = a.targets[t];
                 const int ix = L / a.nby, iy = L - ix * a.nby;
@@ -100,6 +101,8 @@ __global__ void __launch_bounds__(NT, 1) k_windows(const KArgs a) {
         WinStat *st;
         double *out;
         const double *corr = nullptr;
+        // mode 2: job 0 solves the forward window, job 1 its adjoint on the same window state
+        const bool adjoint = a.mode == 2 && job == 1;
         if (a.mode == 1) {
             kind = item == 0 ? KIND_CORR_BLOCK : KIND_CORR_NULL;
             st = a.stat + item;
@@ -107,25 +110,50 @@ __global__ void __launch_bounds__(NT, 1) k_windows(const KArgs a) {
         } else {
             // the landscape window, then the flow potential: conductance 1 on the whole rectangle
             // (omniscape.cpp:127-166), with the sources the landscape pass scaled
-            kind = job == 0 ? KIND_LAND : KIND_FLOW;
+            kind = (a.mode == 0 && job == 1) ? KIND_FLOW : KIND_LAND;
             st = a.stat + 2 * static_cast<int64_t>(t) + job;
             out = (job == 0 ? a.cur_win : a.fp_win) + static_cast<size_t>(item) * W * W;
             corr = a.correct ? a.corr : nullptr;
         }
         ++job;
-        win.mark(PH_OTHER);
-        win.load(kind, kind == KIND_LAND ? a.lat_amps[L] : 0.0);
-        if (kind == KIND_LAND && a.cond_present[0]) win.apply_conditions(a.cond_val[2 * t], a.cond_val[2 * t + 1]);
-        win.mark(PH_LOAD);
-        const bool ok = win.flood(kind);
-        win.mark(PH_FLOOD);
-        if (ok && win.mark_unknowns() != 0.0) {
-            win.mark(PH_MARK);
-            win.assemble();
-            win.solve(st);
-            win.currents(out, corr, cy0, cx0);
-        } else if (threadIdx.x == 0) {
-            *st = WinStat{0, 0, 0, 0.f};
+        bool solvable;
+        if (adjoint) {
+            solvable = adj_go;
+        } else {
+            win.mark(PH_OTHER);
+            win.load(kind, kind == KIND_LAND ? a.lat_amps[L] : 0.0);
+            if (kind == KIND_LAND && a.cond_present[0]) win.apply_conditions(a.cond_val[2 * t], a.cond_val[2 * t + 1]);
+            win.mark(PH_LOAD);
+            const bool ok = win.flood(kind);
+            win.mark(PH_FLOOD);
+            solvable = ok && win.mark_unknowns() != 0.0;
+            if (solvable) {
+                win.mark(PH_MARK);
+                win.assemble();
+            }
+        }
+        if (solvable) {
+            win.solve(st, !adjoint);
+            if (a.mode != 2) {
+                win.currents(out, corr, cy0, cx0);
+            } else if (!adjoint) {
+                bool any = false;
+                const double J = win.adjoint_prep(&any);
+                if (threadIdx.x == 0) {
+                    a.Jw[t] = J;
+                    if (!any) st->status = 0;  // no gradient window: the gather skips it
+                }
+                adj_go = any;
+            } else {
+                win.grad_finish(a.cur_win + static_cast<size_t>(item) * W * W,
+                                a.fp_win + static_cast<size_t>(item) * W * W, a.lat_amps[L]);
+            }
+        } else {
+            if (threadIdx.x == 0) {
+                *st = WinStat{0, 0, 0, 0.f};
+                if (a.mode == 2 && !adjoint) a.Jw[t] = 0.0;
+            }
+            if (a.mode == 2 && !adjoint) adj_go = false;
         }
     }
 #ifdef LSB_PHASE_TIMERS

@@ -7,7 +7,8 @@ All rasters are float64, row-major, NaN = NoData, drawn with ``numpy.random.defa
 * ``omni_1024`` -- 1024 x 1024 Gaussian random field g (power spectrum ~ |k|^-3, rescaled to [0, 1]),
   resistance 10^(2 g) in [1, 100], about 1% NoData as random 3 x 3 clusters, source 1 where g < 0.3;
   radius 32, block 3.
-* ``adjoint_512`` -- 512 x 512, the field and sources of ``omni_1024``; radius 24, block 1; J = sum of the
+* ``adjoint_512`` -- 512 x 512, the resistance of ``omni_1024`` (field, 1% NoData clusters), Omniscape's
+  default sources 1 / resistance (held fixed when differentiating); radius 24, block 1; J = sum of the
   cumulative current over rows and columns 224-287.
 * ``omni_4096`` -- 4096 x 4096 field with exponent -2.5, resistance 500^g in [1, 500], 5% NoData as random
   polygons, source 1 / resistance above the 40th percentile of resistance, else 0; radius 64, block 5.
@@ -96,7 +97,8 @@ def omni_1024(seed: int = 0):
 
 
 def adjoint_512(seed: int = 0):
-    r, s = omni_grf(512, seed)
+    r, _ = omni_grf(512, seed)
+    s = np.where(np.isnan(r), 0.0, 1.0 / np.nan_to_num(r, nan=1.0))  # Omniscape's default sources, 1 / resistance
     weight = np.zeros(r.shape)
     weight[224:288, 224:288] = 1.0
     return r, s, weight, dict(radius=24, block_size=1, buffer=0, four_neighbors=False)
