@@ -1,21 +1,26 @@
 """Benchmark of the Omniscape moving-window solve on B200 (one JSON line on rank 0).
 
 Workload (``omni_1024``): 1024 x 1024 Gaussian-random-field resistance 10^(2g) with ~1% NoData in 3 x 3
-clusters, source 1 where g < 0.3; radius 32, block 3, 8 neighbours, average-conductance edges; cumulative
-current.  A step is one full Omniscape run over the raster (every target window solved and scattered).
+clusters, source 1 where g < 0.3; radius 32, block 3, 8 neighbours, average-conductance edges, block-artifact
+correction on; cumulative current.  A step is one full Omniscape run over the raster (every target window solved
+and scattered).
 
 * ``value``: windows/s of the FP32-CG + FP64-refinement solve with the rasters resident in HBM, device time
   (CUDA events), L2 flushed between steps, max over ranks; every rank solves its own seeded raster (weak
   scaling, no collective on the data path).
 * ``e2e``: the same metric through the drop-in ``landschaft_b200.omniscape(numpy, ...)`` call: host rasters
   in, host maps out, the copies inside the timed region.
-* ``fp64``: the plain FP64 Jacobi-PCG GPU path on the same workload; ``fp32_over_fp64`` their ratio;
-  ``max_rel_err_vs_fp64``: max relative difference of the cumulative currents of the two solves (cells above
-  1e-12 of the maximum).
-* ``cpu_baseline``: the reference's own driver (oracle/_ref, else the C restatement) on the host cores, on a
-  bounded sample of the targets (rank 0, N = 1).
+* ``fp64``: the plain FP64 Jacobi-PCG GPU path on the same workload; ``fp32_over_fp64`` their ratio.
+* ``max_rel_err``: max relative error of the cumulative current over the cells above 1e-12 of the maximum,
+  against the reference's own driver (oracle/_ref, FP64 direct solves) on the whole map, for both GPU solvers;
+  also FP32 against FP64.
+* ``cpu_baseline``: that reference run, timed on the host cores (rank 0, N = 1).
+* ``roofline``: the window kernel's algorithmic HBM bytes (32 B per window cell: resistance and source read,
+  current read and written) over its event time; ``smem``: its algorithmic shared-memory bytes per CG
+  iteration (84 B per unknown) over the same time.
 
-``--impl reference`` times that CPU reference alone, each step a bounded sample.
+``--impl reference`` times that CPU reference alone, each step one run over the whole map.
+``--profile-run`` runs the FP32 solve once (optionally on a centred ``--crop``), for profiler captures.
 """
 
 from __future__ import annotations
@@ -38,6 +43,10 @@ sys.path.insert(0, str(ROOT))
 METRIC = "Omniscape windows/s: batched FP32+refine vs plain FP64 GPU, at <=1e-6 rel err"
 WORKLOAD = {"workload": "omni_1024", "raster": "1024x1024", "radius": 32, "block_size": 3, "buffer": 0,
             "neighbours": 8, "edge_weights": "average", "outputs": "cum_currmap"}
+
+
+SMEM_BYTES_PER_CYCLE = 128  # shared-memory bandwidth of one SM
+SMS = 148
 
 
 def peaks():
@@ -148,31 +157,19 @@ class Clocks:
 # the CPU reference (bounded sample)
 # ---------------------------------------------------------------------------------------------------------------
 
-def cpu_sample(r, s, kw, target_windows=1000):
-    """Sources kept only in a central square, grown until it holds about `target_windows` targets."""
-    import oracle
-    ny, nx = r.shape
-    bs = kw["block_size"]
-    side = 2 * bs
-    while True:
-        y0, x0 = (ny - side) // 2, (nx - side) // 2
-        ss = np.zeros_like(s)
-        ss[y0:y0 + side, x0:x0 + side] = s[y0:y0 + side, x0:x0 + side]
-        n = oracle.count_targets(ss, kw["radius"], kw["buffer"], bs)
-        if n >= target_windows or side >= min(nx, ny):
-            break
-        side = min(min(nx, ny), int(side * 1.25) + bs)
-    return ss, n, f"targets of the central {side}x{side} cells of the map ({n} windows, sources outside zeroed)"
-
-
 def run_cpu_reference(r, s, kw, threads):
+    """The reference's own driver (oracle/_ref; else the C restatement) over the whole map: (seconds, windows,
+    kind, cumulative current)."""
     import oracle
     kind = "reference" if oracle.REF_AVAILABLE else "port"
     t0 = time.perf_counter()
     out = oracle.core_omniscape(r, s, kw["radius"], kw["buffer"], kw["block_size"], False, False, True, False,
                                 threads=threads, impl="ref" if kind == "reference" else "port")
     dt = time.perf_counter() - t0
-    return dt, out["n_targets"], kind
+    return dt, out["n_targets"], kind, out["current"]
+
+
+SAMPLE = "the whole map, every target window (FP64 direct solves)"
 
 
 # ---------------------------------------------------------------------------------------------------------------
@@ -183,6 +180,11 @@ def max_rel(ours, want):
     top = np.nanmax(np.abs(want))
     m = ~np.isnan(want) & (np.abs(want) > 1e-12 * top)
     return float(np.max(np.abs(ours[m] - want[m]) / np.abs(want[m]))) if m.any() else 0.0
+
+
+def patterns_match(ours, want):
+    """NaN and zero cells in the same places."""
+    return bool(np.array_equal(np.isnan(ours), np.isnan(want)) and np.array_equal(ours == 0, want == 0))
 
 
 def time_device(lsb_om, rt, st, params, steps, warmup, flush):
@@ -227,6 +229,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--workload", default="omni_1024")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--crop", type=int, default=0, help="centred square crop of the workload (profile runs)")
+    ap.add_argument("--profile-run", action="store_true", help="one FP32 solve of the workload and exit")
     args = ap.parse_args()
     rank, world, local = dist_env()
     from landschaft_b200 import synthetic
@@ -235,12 +239,11 @@ def main():
         if rank != 0:
             return
         r, s, kw = synthetic.omni_1024(0)
-        ss, n, sample = cpu_sample(r, s, kw, target_windows=1000)
         threads = os.cpu_count() or 1
         times = []
         kind = None
         for i in range(args.warmup + args.steps):
-            dt, nt, kind = run_cpu_reference(r, ss, kw, threads)
+            dt, n, kind, _ = run_cpu_reference(r, s, kw, threads)
             if i >= args.warmup:
                 times.append(dt)
         v = n / statistics.mean(times)
@@ -249,7 +252,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded Gaussian random field; no dataset is published for this path)",
                 "config": {**WORKLOAD, "precision": "fp64 direct (CPU)"},
-                "cpu_baseline": {"value": v, "unit": "windows/s", "cores": threads, "kind": kind, "sample": sample},
+                "cpu_baseline": {"value": v, "unit": "windows/s", "cores": threads, "kind": kind, "sample": SAMPLE},
                 "e2e": {"value": v, "unit": "windows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
@@ -261,19 +264,31 @@ def main():
     from landschaft_b200 import omni as lsb_om
 
     r, s, kw = synthetic.WORKLOADS[args.workload](rank)
+    if args.crop:
+        y0, x0 = (r.shape[0] - args.crop) // 2, (r.shape[1] - args.crop) // 2
+        r = np.ascontiguousarray(r[y0:y0 + args.crop, x0:x0 + args.crop])
+        s = np.ascontiguousarray(s[y0:y0 + args.crop, x0:x0 + args.crop])
     dev = torch.device("cuda", local)
     rt = torch.from_numpy(r).to(dev)
     st = torch.from_numpy(s).to(dev)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # 256 MiB > 126 MB L2
     p32 = lsb_om.make_params(kw["radius"], kw["buffer"], kw["block_size"], solver="fp32-refine")
     p64 = lsb_om.make_params(kw["radius"], kw["buffer"], kw["block_size"], solver="fp64", preconditioner="jacobi")
+    if args.profile_run:
+        p = lsb_om.make_params(kw["radius"], kw["buffer"], kw["block_size"], solver="fp32-refine", use_graph=False)
+        _, stats = lsb_om.run_device(rt, st, p)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_run": args.workload, "crop": args.crop, "windows": int(stats.n_targets),
+                          "cg_iterations_mean": stats.iters_total / max(stats.n_solved, 1)}), flush=True)
+        d.close()
+        return
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # 256 MiB > 126 MB L2
     # correctness and counts (outside the timed region)
     out32, stats32 = lsb_om.run_device(rt, st, p32)
     c32 = out32["current"].cpu().numpy()
     out64, stats64 = lsb_om.run_device(rt, st, p64)
     c64 = out64["current"].cpu().numpy()
     n_windows = int(stats32.n_targets)
-    err = max_rel(c32, c64)
+    err = {"fp32_vs_fp64": max_rel(c32, c64)}
     lsb_om.run_device(rt, st, p32)
     launches = int(lsb_om.last_launch_count())
 
@@ -309,18 +324,23 @@ def main():
     active = lsb_om.active_blocks(s, kw["block_size"])
     assert int(active.sum()) == n_windows
     cells = lsb_om.window_cells(r.shape, {**kw, "active": active})  # sum over targets of the window box cells
-    hbm_bytes = cells * 24.0  # per window cell: resistance 8 + source 8 read, current 8 written
+    hbm_bytes = cells * 32.0  # per window cell: resistance 8 + source 8 read, current 8 read + 8 written
     peak, peak_kind = peaks()
     achieved = hbm_bytes / ktime / 1e9
     prof = ROOT / "profiles" / "k_windows_omni_1024_traffic.json"
-    traffic = json.loads(prof.read_text())["dram_bytes_per_launch"] if prof.exists() else None
+    traffic = json.loads(prof.read_text())["dram_bytes_per_launch"] if prof.exists() and not args.crop else None
+    smem_bytes = kstats.unknown_iters * 84.0  # per unknown and CG iteration (FP32, 8 neighbours)
+    smem_peak = SMEM_BYTES_PER_CYCLE * SMS * (clk["sm_mhz"] or 1965.0) * 1e6 / 1e9
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        ss, n, sample = cpu_sample(r, s, kw, target_windows=1000)
         threads = os.cpu_count() or 1
-        dt, nt, kind = run_cpu_reference(r, ss, kw, threads)
-        cpu = {"value": n / dt, "unit": "windows/s", "cores": threads, "kind": kind, "sample": sample}
+        dt, n, kind, cref = run_cpu_reference(r, s, kw, threads)
+        assert n == n_windows
+        cpu = {"value": n / dt, "unit": "windows/s", "cores": threads, "kind": kind, "sample": SAMPLE}
+        err["fp32_vs_reference"] = max_rel(c32, cref)
+        err["fp64_vs_reference"] = max_rel(c64, cref)
+        err["nan_and_zero_patterns_match"] = patterns_match(c32, cref) and patterns_match(c64, cref)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "windows/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1e3 * T32 / args.steps, "higher_is_better": True,
@@ -334,7 +354,7 @@ def main():
                 "fp64": {"value": fp64_value, "unit": "windows/s", "preconditioner": "jacobi",
                          "ms_per_step": 1e3 * T64},
                 "fp32_over_fp64": value / fp64_value,
-                "max_rel_err_vs_fp64": err,
+                "max_rel_err": err,
                 "cg_iterations": {"fp32_mean": stats32.iters_total / max(stats32.n_solved, 1),
                                   "fp32_max": stats32.iters_max, "refine_max": stats32.refine_max,
                                   "fp64_mean": stats64.iters_total / max(stats64.n_solved, 1),
@@ -343,8 +363,12 @@ def main():
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                              "kernel": "k_windows", "kernel_ms": ktime * 1e3,
-                             "note": "algorithmic HBM bytes (24 B per window cell) over the window kernel's "
+                             "note": "algorithmic HBM bytes (32 B per window cell) over the window kernel's "
                                      "event time; the solve itself runs out of shared memory"},
+                "smem": {"achieved": smem_bytes / ktime / 1e9, "peak": smem_peak, "unit": "GB/s",
+                         "frac": smem_bytes / ktime / 1e9 / smem_peak,
+                         "note": "84 B per unknown and CG iteration over the window kernel's event time; peak = "
+                                 "128 B/cycle/SM x 148 SMs x the median SM clock (nominal)"},
                 "clocks": clk, "gpu_launches": launches * args.steps, "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
     d.close()

@@ -102,6 +102,7 @@ typedef struct lsb_omni_stats {
     int32_t pad_;
     double worst_residual;  /* largest final relative FP64 residual */
     double window_ms;       /* device time of the window-solve kernels (see lsb_time_window_kernels) */
+    double unknown_iters;   /* sum over solves of unknowns x CG iterations (the inner solve's work) */
 } lsb_omni_stats;
 
 /* Fill the defaults: radius 0, buffer 0, block 1, average weights, correction

@@ -42,7 +42,8 @@ class Stats(C.Structure):
     _fields_ = [("n_targets", C.c_int64), ("n_solved", C.c_int64), ("n_failed", C.c_int64),
                 ("iters_total", C.c_int64), ("iters_max", C.c_int32), ("refine_max", C.c_int32),
                 ("batches", C.c_int32), ("threads_per_window", C.c_int32), ("preconditioner", C.c_int32),
-                ("pad_", C.c_int32), ("worst_residual", C.c_double), ("window_ms", C.c_double)]
+                ("pad_", C.c_int32), ("worst_residual", C.c_double), ("window_ms", C.c_double),
+                ("unknown_iters", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad_"}

@@ -615,6 +615,7 @@ int lsb_omniscape(const double *resistance, const double *source, int64_t nx, in
         stats->threads_per_window = pl.v.nt;
         stats->preconditioner = resolved_pc(p);
         stats->worst_residual = ds.worst_residual;
+        stats->unknown_iters = ds.unknown_iters;
         if (hdr[1]) {
             set_err(err, errlen, "a target block has no value of a condition (all NoData)");
             return LSB_ERR_CONDITION;
@@ -900,6 +901,7 @@ int lsb_omniscape_grad(const double *resistance, const double *source, const dou
         stats->threads_per_window = pl.v.nt;
         stats->preconditioner = resolved_pc(p);
         stats->worst_residual = ds.worst_residual;
+        stats->unknown_iters = ds.unknown_iters;
         if (ds.n_failed > 0) {
             set_err(err, errlen, "%lld window solves of the adjoint did not converge (worst relative residual %.3g)",
                     static_cast<long long>(ds.n_failed), ds.worst_residual);

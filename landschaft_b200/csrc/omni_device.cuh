@@ -143,6 +143,7 @@ struct WinStat {
     int outer;
     int status;  // 0 no solve needed, 1 converged, 2 not converged, 3 breakdown / non-finite
     float resid;  // final relative FP64 residual
+    int nu;       // unknowns of the system
 };
 
 // ---------------------------------------------------------------------------

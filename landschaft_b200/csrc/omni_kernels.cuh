@@ -302,6 +302,7 @@ struct DevStats {
     long long n_solved, n_failed, iters_total;
     int iters_max, refine_max;
     double worst_residual;
+    double unknown_iters;
 };
 
 __global__ void __launch_bounds__(1024) k_stats(const WinStat *__restrict__ st, const int *__restrict__ count_ptr,
@@ -309,19 +310,20 @@ __global__ void __launch_bounds__(1024) k_stats(const WinStat *__restrict__ st, 
     __shared__ double red_buf[128];
     Reducer<1024> red{red_buf, 0};
     const int n = *count_ptr * per_target;
-    double solved = 0, failed = 0, iters = 0, imax = 0, omax = 0, rmax = 0;
+    double solved = 0, failed = 0, iters = 0, imax = 0, omax = 0, rmax = 0, ui = 0;
     for (int i = threadIdx.x; i < n; i += 1024) {
         const WinStat s = st[i];
         if (s.status == 0) continue;
         solved += 1;
         failed += s.status >= 2 ? 1 : 0;
         iters += s.iters;
+        ui += static_cast<double>(s.iters) * s.nu;
         imax = fmax(imax, static_cast<double>(s.iters));
         omax = fmax(omax, static_cast<double>(s.outer));
         rmax = fmax(rmax, static_cast<double>(s.resid));
     }
     red.sum2(solved, failed);
-    iters = red.sum(iters);
+    red.sum2(iters, ui);
     red.max2(imax, omax);
     rmax = red.max(rmax);
     if (threadIdx.x == 0) {
@@ -331,6 +333,7 @@ __global__ void __launch_bounds__(1024) k_stats(const WinStat *__restrict__ st, 
         out->iters_max = static_cast<int>(imax);
         out->refine_max = static_cast<int>(omax);
         out->worst_residual = rmax;
+        out->unknown_iters = ui;
     }
 }
 

@@ -1140,6 +1140,7 @@ struct Win {
             st->outer = outer;
             st->status = status;
             st->resid = static_cast<float>(rel);
+            st->nu = nu;
         }
     }
 

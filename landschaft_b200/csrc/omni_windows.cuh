@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(NT, 1) k_windows(const KArgs a) {
             }
         } else {
             if (threadIdx.x == 0) {
-                *st = WinStat{0, 0, 0, 0.f};
+                *st = WinStat{0, 0, 0, 0.f, 0};
                 if (a.mode == 2 && !adjoint) a.Jw[t] = 0.0;
             }
             if (a.mode == 2 && !adjoint) adj_go = false;
