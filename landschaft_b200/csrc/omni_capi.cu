@@ -199,14 +199,19 @@ ArenaLayout make_layout(const Variant &v, int W, size_t smem_budget, bool grad) 
     }
     L.smem_bytes = static_cast<uint32_t>(so);
     L.gmem_bytes = static_cast<uint32_t>(align_up(go));
+    L.hot = 1;
+    for (const Item &it : items)
+        if (hot_array(it.arr) && (L.off[it.arr] & 0x80000000u)) L.hot = 0;
     return L;
 }
 
 // ---------------------------------------------------------------------------
 // Kernel dispatch.
 // ---------------------------------------------------------------------------
-KernelFn pick(const Variant &v) {
-    return v.nt == 256 ? pick_windows_256(v.four, v.dbl, v.mg) : pick_windows_512(v.four, v.dbl, v.mg);
+KernelFn pick(const Variant &v, bool hot) {
+    if (v.nt == 256)
+        return hot ? pick_windows_256_hot(v.four, v.dbl, v.mg) : pick_windows_256_gen(v.four, v.dbl, v.mg);
+    return hot ? pick_windows_512_hot(v.four, v.dbl, v.mg) : pick_windows_512_gen(v.four, v.dbl, v.mg);
 }
 
 struct DeviceInfo {
@@ -260,7 +265,7 @@ int make_plan(int64_t nx, int64_t ny, const lsb_omni_params *p, Plan *pl, char *
     LSB_CK(device_info(&di));
     const size_t budget = di.smem_optin > kStaticSmem ? di.smem_optin - kStaticSmem : 0;
     pl->lay = make_layout(pl->v, g.W, budget, grad);
-    pl->kern = pick(pl->v);
+    pl->kern = pick(pl->v, pl->lay.hot != 0);
     LSB_CK(cudaFuncSetAttribute(reinterpret_cast<const void *>(pl->kern),
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(pl->lay.smem_bytes)));
     int per_sm = 0;
@@ -592,7 +597,9 @@ int lsb_omniscape(const double *resistance, const double *source, int64_t nx, in
             LSB_CK(cudaMemcpy(tm, ws + pl.o_timers, sizeof tm, cudaMemcpyDeviceToHost));
             static const char *names[PH_COUNT] = {"load", "flood", "mark", "assemble", "mg_setup", "resid64", "cg",
                                                   "vcycle", "currents", "other", "v_pre0", "v_restrict1", "v_down",
-                                                  "v_coarsest", "v_up", "v_prolong0", "v_post0"};
+                                                  "v_coarsest", "v_up", "v_prolong0", "v_post0",
+                                                  "ds1", "ds2", "ds3", "dr1", "dr2", "dr3", "up1", "up2", "up3",
+                                                  "us1", "us2", "us3"};
             double tot = 0;
             for (int k = 0; k < PH_COUNT; ++k) tot += static_cast<double>(tm[k]);
             fprintf(stderr, "[phases] windows=%d cycles/window:", hdr[0]);

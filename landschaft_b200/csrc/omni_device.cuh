@@ -125,6 +125,7 @@ struct ArenaLayout {
     uint32_t off[AR_COUNT];
     uint32_t smem_bytes;
     uint32_t gmem_bytes;  // per CTA
+    uint32_t hot;         // 1: every array but the FP64 window arrays is in shared memory
 };
 
 // Solver configuration for one launch.

@@ -49,7 +49,10 @@ struct KArgs {
 // Phases of a window solve, for the cycle counters of profiling builds.
 enum Phase : int { PH_LOAD = 0, PH_FLOOD, PH_MARK, PH_ASSEMBLE, PH_MG_SETUP, PH_RESID, PH_CG, PH_VCYCLE, PH_CURRENTS,
                    PH_OTHER, PH_V_PRE0, PH_V_RESTRICT1, PH_V_DOWN, PH_V_COARSEST, PH_V_UP, PH_V_PROLONG0, PH_V_POST0,
-                   PH_COUNT };
+                   // levels 1-3 (deeper levels count as 3): down smoothing, restriction; up prolongation, smoothing
+                   PH_L_DS, PH_L_DR = PH_L_DS + 3, PH_L_UP = PH_L_DR + 3, PH_L_US = PH_L_UP + 3,
+                   PH_COUNT = PH_L_US + 3 };
+static_assert(PH_COUNT <= 30, "two timer slots are calibration");
 
 template <typename X>
 __device__ __forceinline__ X *arena_ptr(const ArenaLayout &L, int a, char *sm, char *gm) {
@@ -104,7 +107,14 @@ __device__ __forceinline__ int block_compact(int n, F flag, uint16_t *out, int *
 // ---------------------------------------------------------------------------
 // The solver of one window.
 // ---------------------------------------------------------------------------
-template <int NT, typename T, bool FOUR, bool MG, bool REFINE>
+// Arrays a window keeps in shared memory whenever the layout's HOT flag is set: all but the FP64 window arrays.
+__host__ __device__ constexpr bool hot_array(int k) {
+    return !(k == AR_X64 || k == AR_G64 || k == AR_B64 || k == AR_V64 || k == AR_CW || k == AR_DG64);
+}
+
+// HOT: every hot array of the layout is in shared memory, so their pointers derive from the shared-memory base and
+// compile to 32-bit shared addressing (else each pointer is chosen at run time and addressed generically).
+template <int NT, typename T, bool FOUR, bool MG, bool REFINE, bool HOT>
 struct Win {
     using NB = Nb<FOUR>;
     static constexpr int ND = NB::ND, LOWER = NB::LOWER;
@@ -114,6 +124,7 @@ struct Win {
     Reducer<NT> &red;
     int *scan;       // shared scratch (>= 64 ints)
     int *lvh, *lvw;  // shared: level dimensions
+    float *lvinv;    // shared: 1 / level width
     short *cidx;     // shared: padded indices of the coarsest level's cells (kNcMax)
     float invP = 1.f;  // 1 / G.P
     WinGeom G;
@@ -139,13 +150,17 @@ struct Win {
     }
 
     __device__ Win(const KArgs &a_, char *sm_, char *gm_, Reducer<NT> &red_, int *scan_, int *lvh_, int *lvw_,
-                   short *cidx_)
-        : a(a_), sm(sm_), gm(gm_), red(red_), scan(scan_), lvh(lvh_), lvw(lvw_), cidx(cidx_) {}
+                   float *lvinv_, short *cidx_)
+        : a(a_), sm(sm_), gm(gm_), red(red_), scan(scan_), lvh(lvh_), lvw(lvw_), lvinv(lvinv_), cidx(cidx_) {}
 
     template <typename X>
-    __device__ __forceinline__ X *A(int k) const { return arena_ptr<X>(a.lay, k, sm, gm); }
+    __device__ __forceinline__ X *A(int k) const {
+        if (HOT && hot_array(k)) return reinterpret_cast<X *>(sm + a.lay.off[k]);
+        return arena_ptr<X>(a.lay, k, sm, gm);
+    }
     template <typename X>
     __device__ __forceinline__ X *LV(int l, int k) const {
+        if (HOT) return reinterpret_cast<X *>(sm + a.lay.off[AR_LEVEL + (l - 1) * LV_COUNT + k]);
         return arena_ptr<X>(a.lay, AR_LEVEL + (l - 1) * LV_COUNT + k, sm, gm);
     }
     __device__ __forceinline__ int noff(int d) const { return NB::dy(d) * G.P + NB::dx(d); }
@@ -446,7 +461,7 @@ struct Win {
     template <class F>
     __device__ __forceinline__ void for_cells(int l, F f) const {
         const int h = lvh[l], w = lvw[l], P = w + 2, n = h * w;
-        const float invw = 1.0f / static_cast<float>(w);
+        const float invw = lvinv[l];
         for (int k = threadIdx.x; k < n; k += NT) {
             const int y = static_cast<int>((static_cast<float>(k) + 0.5f) * invw), x = k - y * w;
             f(y, x, (y + 1) * P + x + 1);
@@ -554,6 +569,7 @@ struct Win {
             for (int l = 0; l < nlev; ++l) {
                 lvh[l] = h;
                 lvw[l] = w;
+                lvinv[l] = 1.0f / static_cast<float>(w);
                 h = coarse_dim(h);
                 w = coarse_dim(w);
             }
@@ -745,7 +761,9 @@ struct Win {
                 t[i] = b[i] - s;
             });
             __syncthreads();
+            mark(PH_L_DS + (l < 3 ? l : 3) - 1);
             restrict_to(l + 1, t);
+            mark(PH_L_DR + (l < 3 ? l : 3) - 1);
         }
         mark(PH_V_DOWN);
         coarse_solve(nlev - 1, LV<T>(nlev - 1, LV_B), LV<T>(nlev - 1, LV_X));
@@ -758,11 +776,13 @@ struct Win {
             const T *xc = LV<T>(l + 1, l + 1 == nlev - 1 ? LV_X : LV_T);
             prolong_add(l, x, xc);
             __syncthreads();
+            mark(PH_L_UP + (l < 3 ? l : 3) - 1);
             for_cells(l, [&](int, int, int i) {
                 const T ivi = iv[i];
                 if (ivi != T(0)) t[i] = x[i] + ivi * (b[i] - applyc(L, x, i));
             });
             __syncthreads();
+            mark(PH_L_US + (l < 3 ? l : 3) - 1);
         }
         mark(PH_V_UP);
         prolong_add(0, z, LV<T>(1, nlev - 1 == 1 ? LV_X : LV_T));
@@ -968,6 +988,7 @@ struct Win {
                     d[i] += alpha * p[i];
                     r[i] -= alpha * q[i];
                 }
+                __syncthreads();  // the pre-smoothing reads r at the neighbours
                 mark(PH_CG);
                 vcycle(r);
                 mark(PH_VCYCLE);

@@ -13,17 +13,18 @@ using KernelFn = void (*)(const KArgs);
 // ---------------------------------------------------------------------------
 // The persistent window solver.
 // ---------------------------------------------------------------------------
-template <int NT, typename T, bool FOUR, bool MG, bool REFINE>
+template <int NT, typename T, bool FOUR, bool MG, bool REFINE, bool HOT>
 __global__ void __launch_bounds__(NT, 1) k_windows(const KArgs a) {
     extern __shared__ __align__(16) char smem[];
     __shared__ double red_buf[128];
     __shared__ int scan_buf[64];
     __shared__ int lvh[kMaxLevels], lvw[kMaxLevels];
+    __shared__ float lvinv[kMaxLevels];
     __shared__ short cidx[kNcMax];
     __shared__ int item_s;
     char *gm = a.gscratch + static_cast<size_t>(blockIdx.x) * a.lay.gmem_bytes;
     Reducer<NT> red{red_buf, 0};
-    Win<NT, T, FOUR, MG, REFINE> win(a, smem, gm, red, scan_buf, lvh, lvw, cidx);
+    Win<NT, T, FOUR, MG, REFINE, HOT> win(a, smem, gm, red, scan_buf, lvh, lvw, lvinv, cidx);
 #ifdef LSB_PHASE_TIMERS
     __shared__ unsigned long long tacc[PH_COUNT + 1];
     if (threadIdx.x <= PH_COUNT) tacc[threadIdx.x] = threadIdx.x == PH_COUNT ? clock64() : 0ull;
@@ -163,18 +164,21 @@ __global__ void __launch_bounds__(NT, 1) k_windows(const KArgs a) {
 }
 
 
-// One translation unit per block size instantiates the variants of that size.
-KernelFn pick_windows_256(bool four, bool dbl, bool mg);
-KernelFn pick_windows_512(bool four, bool dbl, bool mg);
+// One translation unit per block size and layout kind instantiates the variants of that kind.
+KernelFn pick_windows_256_hot(bool four, bool dbl, bool mg);
+KernelFn pick_windows_256_gen(bool four, bool dbl, bool mg);
+KernelFn pick_windows_512_hot(bool four, bool dbl, bool mg);
+KernelFn pick_windows_512_gen(bool four, bool dbl, bool mg);
 
-template <int NT>
+template <int NT, bool HOT>
 KernelFn pick_windows_nt(bool four, bool dbl, bool mg) {
     if (four) {
-        if (dbl) return mg ? k_windows<NT, double, true, true, false> : k_windows<NT, double, true, false, false>;
-        return mg ? k_windows<NT, float, true, true, true> : k_windows<NT, float, true, false, true>;
+        if (dbl)
+            return mg ? k_windows<NT, double, true, true, false, HOT> : k_windows<NT, double, true, false, false, HOT>;
+        return mg ? k_windows<NT, float, true, true, true, HOT> : k_windows<NT, float, true, false, true, HOT>;
     }
-    if (dbl) return mg ? k_windows<NT, double, false, true, false> : k_windows<NT, double, false, false, false>;
-    return mg ? k_windows<NT, float, false, true, true> : k_windows<NT, float, false, false, true>;
+    if (dbl) return mg ? k_windows<NT, double, false, true, false, HOT> : k_windows<NT, double, false, false, false, HOT>;
+    return mg ? k_windows<NT, float, false, true, true, HOT> : k_windows<NT, float, false, false, true, HOT>;
 }
 
 }  // namespace lsb
