@@ -125,6 +125,7 @@ struct Win {
     int *scan;       // shared scratch (>= 64 ints)
     int *lvh, *lvw;  // shared: level dimensions
     float *lvinv;    // shared: 1 / level width
+    uint32_t *lvoff; // shared: arena offsets of the coarse levels' arrays, LV_COUNT per level (from level 1)
     short *cidx;     // shared: padded indices of the coarsest level's cells (kNcMax)
     float invP = 1.f;  // 1 / G.P
     WinGeom G;
@@ -150,18 +151,22 @@ struct Win {
     }
 
     __device__ Win(const KArgs &a_, char *sm_, char *gm_, Reducer<NT> &red_, int *scan_, int *lvh_, int *lvw_,
-                   float *lvinv_, short *cidx_)
-        : a(a_), sm(sm_), gm(gm_), red(red_), scan(scan_), lvh(lvh_), lvw(lvw_), lvinv(lvinv_), cidx(cidx_) {}
+                   float *lvinv_, uint32_t *lvoff_, short *cidx_)
+        : a(a_), sm(sm_), gm(gm_), red(red_), scan(scan_), lvh(lvh_), lvw(lvw_), lvinv(lvinv_), lvoff(lvoff_),
+          cidx(cidx_) {}
 
     template <typename X>
     __device__ __forceinline__ X *A(int k) const {
         if (HOT && hot_array(k)) return reinterpret_cast<X *>(sm + a.lay.off[k]);
         return arena_ptr<X>(a.lay, k, sm, gm);
     }
+    // (the offsets come from the shared table: a level index known only at run time would otherwise index the
+    // kernel's parameters)
     template <typename X>
     __device__ __forceinline__ X *LV(int l, int k) const {
-        if (HOT) return reinterpret_cast<X *>(sm + a.lay.off[AR_LEVEL + (l - 1) * LV_COUNT + k]);
-        return arena_ptr<X>(a.lay, AR_LEVEL + (l - 1) * LV_COUNT + k, sm, gm);
+        const uint32_t o = lvoff[(l - 1) * LV_COUNT + k];
+        if (HOT) return reinterpret_cast<X *>(sm + o);
+        return reinterpret_cast<X *>((o & 0x80000000u) ? gm + (o & 0x7fffffffu) : sm + o);
     }
     __device__ __forceinline__ int noff(int d) const { return NB::dy(d) * G.P + NB::dx(d); }
 
@@ -351,10 +356,36 @@ struct Win {
                 const int n = i + noff(dd);
                 if (mask[n] & M_PRESENT) diag += edge_w64(gi, g64[n], NB::diag(dd), series);
             }
-            invd[i] = static_cast<T>(1.0 / (diag + kShift));
+            // multigrid kernels keep omega / diag: the damped-Jacobi smoother's factor (a scalar multiple of
+            // the Jacobi preconditioner, to which CG is invariant)
+            invd[i] = static_cast<T>((MG ? static_cast<double>(a.sp.omega) : 1.0) / (diag + kShift));
             if (MG) z[i] = static_cast<T>(diag);
         }
         __syncthreads();
+    }
+
+    // Two values of a cell, computed before either is stored.
+    struct TPair {
+        T a, b;
+    };
+    struct DPair {
+        double a, b;
+    };
+
+    // Visits the unknowns k = threadIdx.x + j NT (increasing j, so per-thread sums keep their order) two at a
+    // time: both cells' loads and arithmetic (`calc`, which only reads) come before both stores (`put`), so
+    // the two cells' memory latencies overlap.
+    template <class C, class Put>
+    __device__ __forceinline__ void unknowns2(C calc, Put put) const {
+        const uint16_t *ul = A<uint16_t>(AR_ULIST);
+        for (int k = threadIdx.x; k < nu; k += 2 * NT) {
+            const bool two = k + NT < nu;
+            const int i1 = ul[k], i2 = two ? ul[k + NT] : i1;
+            const auto v1 = calc(i1);
+            const auto v2 = calc(i2);
+            put(i1, v1);
+            if (two) put(i2, v2);
+        }
     }
 
     // ---- level-0 operator in T ---------------------------------------------
@@ -402,6 +433,44 @@ struct Win {
         }
         const T wv = tmax(gT[i] + gT[n], T(0));
         return -(dg ? wv * T(kInvTwoSqrt2) : wv * T(0.5));
+    }
+
+    // The level-0 entries during the multigrid set-up: with precomputed weights (kWeights), the off-diagonal
+    // entries towards E, S, SE and SW of every unknown are held in the (then unused) CG vectors P, Q, R and D,
+    // zero where either end is no unknown; the rest by symmetry.  Same values as entry0.
+    static constexpr bool kWeights = sizeof(T) == 4 || REFINE;  // D exists
+    __device__ __forceinline__ T entry0w(int i, int sy, int sx) const {
+        if (!kWeights) return entry0(i, sy, sx);
+        if (sy == 0 && sx == 0) return A<T>(AR_Z)[i];
+        if (FOUR && sy != 0 && sx != 0) return T(0);
+        const T *WE = A<T>(AR_P), *WS = A<T>(AR_Q), *WSE = A<T>(AR_R), *WSW = A<T>(AR_D);
+        const int P = G.P;
+        if (sy == 0) return sx > 0 ? WE[i] : WE[i - 1];
+        if (sx == 0) return sy > 0 ? WS[i] : WS[i - P];
+        if (sy > 0) return sx > 0 ? WSE[i] : WSW[i];
+        return sx > 0 ? WSW[i - P + 1] : WSE[i - P - 1];
+    }
+    // Fills (fill == true) or clears the weights of entry0w (the vectors are zero before and after).
+    __device__ __forceinline__ void weights0(bool fill) {
+        if (!kWeights) return;
+        T *WE = A<T>(AR_P), *WS = A<T>(AR_Q), *WSE = A<T>(AR_R), *WSW = A<T>(AR_D);
+        unknowns2(
+            [&](int i) { return fill ? TPair{entry0(i, 0, 1), entry0(i, 1, 0)} : TPair{T(0), T(0)}; },
+            [&](int i, const TPair &v) {
+                WE[i] = v.a;
+                WS[i] = v.b;
+            });
+        if (!FOUR) {
+            unknowns2(
+                [&](int i) {
+                    return fill ? TPair{entry0(i, 1, 1), entry0(i, 1, -1)} : TPair{T(0), T(0)};
+                },
+                [&](int i, const TPair &v) {
+                    WSE[i] = v.a;
+                    WSW[i] = v.b;
+                });
+        }
+        __syncthreads();
     }
 
     // The arrays of coarse level l (pointers resolved once, not per cell).
@@ -488,7 +557,7 @@ struct Win {
 #pragma unroll
                     for (int sx = -1; sx <= 1; ++sx) {
                         if (FOUR && L0 && sy != 0 && sx != 0) continue;
-                        const T v = wi * (L0 ? entry0(i, sy, sx) : entryc(F, i, sy, sx));
+                        const T v = wi * (L0 ? entry0w(i, sy, sx) : entryc(F, i, sy, sx));
                         const int dy = ay + sy, dx = ax + sx;  // fine j relative to 2J, in [-2, 2]
 #pragma unroll
                         for (int py = 0; py < 2; ++py) {
@@ -574,6 +643,7 @@ struct Win {
                 w = coarse_dim(w);
             }
         }
+        if (nlev > 1) weights0(true);  // ends with a barrier
         __syncthreads();
         for (int l = 1; l < nlev; ++l) {
             const int hf = lvh[l - 1], wf = lvw[l - 1];
@@ -617,6 +687,7 @@ struct Win {
                 iv[J] = om / acc[0];
             });
             __syncthreads();
+            if (l == 1) weights0(false);
         }
         dense_setup();
     }
@@ -704,10 +775,9 @@ struct Win {
                 }
             }
             __syncwarp();
-            // the inverse is symmetric: row `lane`, columns >= lane (after every lane has read L)
+            // column `lane` of the (symmetric) inverse, after every lane has read L: M holds the full inverse
             if (lane < n)
-                for (int i = 0; i < n; ++i)
-                    if (i >= lane) M[lane * kNcMax + i] = col[i];
+                for (int i = 0; i < n; ++i) M[i * kNcMax + lane] = col[i];
         }
         __syncthreads();
     }
@@ -723,46 +793,31 @@ struct Win {
         const uint16_t *ul = A<uint16_t>(AR_ULIST);
         const T *gT = A<T>(AR_GT), *invd = A<T>(AR_INVD);
         T *z = A<T>(AR_Z), *q = A<T>(AR_Q);
-        const T om = static_cast<T>(a.sp.omega);
         if (nlev == 1) {
             // the window is its own coarsest level
             coarse_solve(0, r, q);
             __syncthreads();
             return;
         }
-        // pre-smoothing from zero and the residual in one pass: z = w D^-1 r, q = r - A z
+        // pre-smoothing from zero and the residual in one pass: z = w D^-1 r, q = r - A z (invd holds w / diag)
         mark(PH_VCYCLE);
-        for (int k = threadIdx.x; k < nu; k += NT) {
-            const int i = ul[k];
-            const T zi = om * invd[i] * r[i];
-            z[i] = zi;
-            q[i] = r[i] - apply0_scaled(gT, r, invd, om, i, zi);
-        }
+        unknowns2(
+            [&](int i) {
+                const T zi = invd[i] * r[i];
+                return TPair{zi, r[i] - apply0_scaled(gT, r, invd, i, zi)};
+            },
+            [&](int i, const TPair &v) {
+                z[i] = v.a;
+                q[i] = v.b;
+            });
         __syncthreads();
         mark(PH_V_PRE0);
         restrict_to(1, q);
         mark(PH_V_RESTRICT1);
         for (int l = 1; l < nlev - 1; ++l) {
-            const Lvl L = lvl(l);
-            T *x = L.x, *t = L.t;
-            const T *b = L.b, *iv = L.iv;
-            const int P = L.P;
-            const T *c0 = L.c0, *cE = L.cE, *cSW = L.cSW, *cS = L.cS, *cSE = L.cSE;
-            for_cells(l, [&](int, int, int i) {
-                const T ivi = iv[i];
-                if (ivi == T(0)) return;
-                auto xv = [&](int j) { return iv[j] * b[j]; };
-                const T xi = ivi * b[i];
-                x[i] = xi;
-                T s = c0[i] * xi;
-                s += cE[i] * xv(i + 1) + cSW[i] * xv(i + P - 1) + cS[i] * xv(i + P) + cSE[i] * xv(i + P + 1);
-                s += cE[i - 1] * xv(i - 1) + cSW[i - P + 1] * xv(i - P + 1) + cS[i - P] * xv(i - P) +
-                     cSE[i - P - 1] * xv(i - P - 1);
-                t[i] = b[i] - s;
-            });
-            __syncthreads();
+            smooth_down(l);
             mark(PH_L_DS + (l < 3 ? l : 3) - 1);
-            restrict_to(l + 1, t);
+            restrict_to(l + 1, LV<T>(l, LV_T));
             mark(PH_L_DR + (l < 3 ? l : 3) - 1);
         }
         mark(PH_V_DOWN);
@@ -770,35 +825,22 @@ struct Win {
         __syncthreads();
         mark(PH_V_COARSEST);
         for (int l = nlev - 2; l >= 1; --l) {
-            const Lvl L = lvl(l);
-            T *x = L.x, *t = L.t;
-            const T *b = L.b, *iv = L.iv;
-            const T *xc = LV<T>(l + 1, l + 1 == nlev - 1 ? LV_X : LV_T);
-            prolong_add(l, x, xc);
-            __syncthreads();
-            mark(PH_L_UP + (l < 3 ? l : 3) - 1);
-            for_cells(l, [&](int, int, int i) {
-                const T ivi = iv[i];
-                if (ivi != T(0)) t[i] = x[i] + ivi * (b[i] - applyc(L, x, i));
-            });
-            __syncthreads();
+            smooth_up(l);
             mark(PH_L_US + (l < 3 ? l : 3) - 1);
         }
         mark(PH_V_UP);
         prolong_add(0, z, LV<T>(1, nlev - 1 == 1 ? LV_X : LV_T));
         __syncthreads();
         mark(PH_V_PROLONG0);
-        for (int k = threadIdx.x; k < nu; k += NT) {
-            const int i = ul[k];
-            q[i] = z[i] + om * invd[i] * (r[i] - apply0(gT, z, i));
-        }
+        unknowns2([&](int i) { return TPair{z[i] + invd[i] * (r[i] - apply0(gT, z, i)), T(0)}; },
+                  [&](int i, const TPair &v) { q[i] = v.a; });
         __syncthreads();
         mark(PH_V_POST0);
     }
 
     // (A z)_i with z_n = w invd_n r_n computed from the neighbours' r (the
     // pre-smoothed iterate without storing it first).
-    __device__ __forceinline__ T apply0_scaled(const T *gT, const T *r, const T *invd, T om, int i, T zi) const {
+    __device__ __forceinline__ T apply0_scaled(const T *gT, const T *r, const T *invd, int i, T zi) const {
         const T gi = gT[i];
         T ao = T(0), ad = T(0);
         if (a.series) {
@@ -806,7 +848,7 @@ struct Win {
             for (int dd = 0; dd < ND; ++dd) {
                 const int n = i + noff(dd);
                 const T wv = T(2) / (gi + gT[n]);
-                const T zn = om * invd[n] * r[n];
+                const T zn = invd[n] * r[n];
                 if (NB::diag(dd))
                     ad += wv * (zi - zn);
                 else
@@ -818,7 +860,7 @@ struct Win {
         for (int dd = 0; dd < ND; ++dd) {
             const int n = i + noff(dd);
             const T wv = tmax(gi + gT[n], T(0));
-            const T zn = om * invd[n] * r[n];
+            const T zn = invd[n] * r[n];
             if (NB::diag(dd))
                 ad += wv * (zi - zn);
             else
@@ -872,7 +914,7 @@ struct Win {
         const int hf = lvh[l], wf = lvw[l], Pf = wf + 2;
         const int hc = lvh[l + 1], wc = lvw[l + 1], Pc = wc + 2;
         const bool cy = hc != hf, cx = wc != wf;
-        auto one = [&](int fy, int fx, int i) {
+        auto interp = [&](int fy, int fx) {
             int y0, y1, x0, x1;
             T wy0, wy1, wx0, wx1;
             if (cy) {
@@ -895,21 +937,20 @@ struct Win {
                 wx0 = T(1);
                 wx1 = T(0);
             }
-            const T v = wy0 * (wx0 * xc[(y0 + 1) * Pc + x0 + 1] + wx1 * xc[(y0 + 1) * Pc + x1 + 1]) +
-                        wy1 * (wx0 * xc[(y1 + 1) * Pc + x0 + 1] + wx1 * xc[(y1 + 1) * Pc + x1 + 1]);
-            x[i] += v;
+            return wy0 * (wx0 * xc[(y0 + 1) * Pc + x0 + 1] + wx1 * xc[(y0 + 1) * Pc + x1 + 1]) +
+                   wy1 * (wx0 * xc[(y1 + 1) * Pc + x0 + 1] + wx1 * xc[(y1 + 1) * Pc + x1 + 1]);
         };
         if (l == 0) {
-            const uint16_t *ul = A<uint16_t>(AR_ULIST);
-            for (int k = threadIdx.x; k < nu; k += NT) {
-                const int i = ul[k];
-                const int py = row0(i);
-                one(py - 1, i - py * Pf - 1, i);
-            }
+            unknowns2(
+                [&](int i) {
+                    const int py = row0(i);
+                    return TPair{x[i] + interp(py - 1, i - py * Pf - 1), T(0)};
+                },
+                [&](int i, const TPair &v) { x[i] = v.a; });
         } else {
             const T *iv = LV<T>(l, LV_INVD);
             for_cells(l, [&](int fy, int fx, int i) {
-                if (iv[i] != T(0)) one(fy, fx, i);
+                if (iv[i] != T(0)) x[i] += interp(fy, fx);
             });
         }
     }
@@ -922,7 +963,7 @@ struct Win {
         const int lane = threadIdx.x & 31;
         const double bv = lane < n ? static_cast<double>(b[cidx[lane]]) : 0.0;
         for (int u = threadIdx.x >> 5; u < n; u += NT / 32) {
-            double s = lane < n ? (lane >= u ? M[u * kNcMax + lane] : M[lane * kNcMax + u]) * bv : 0.0;
+            double s = lane < n ? M[u * kNcMax + lane] * bv : 0.0;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
             if (lane == 0) {
@@ -930,6 +971,43 @@ struct Win {
                 if (l != 0 || (A<uint8_t>(AR_MASK)[iu] & M_UNKNOWN)) x[iu] = static_cast<T>(s);
             }
         }
+    }
+
+    // Down the V-cycle at coarse level l: damped Jacobi from zero (x = iv b) and the residual t = b - A x.
+    __device__ __forceinline__ void smooth_down(int l) {
+        const Lvl L = lvl(l);
+        T *x = L.x, *t = L.t;
+        const T *b = L.b, *iv = L.iv;
+        const int P = L.P;
+        const T *c0 = L.c0, *cE = L.cE, *cSW = L.cSW, *cS = L.cS, *cSE = L.cSE;
+        for_cells(l, [&](int, int, int i) {
+            const T ivi = iv[i];
+            if (ivi == T(0)) return;
+            auto xv = [&](int j) { return iv[j] * b[j]; };
+            const T xi = ivi * b[i];
+            x[i] = xi;
+            T s = c0[i] * xi;
+            s += cE[i] * xv(i + 1) + cSW[i] * xv(i + P - 1) + cS[i] * xv(i + P) + cSE[i] * xv(i + P + 1);
+            s += cE[i - 1] * xv(i - 1) + cSW[i - P + 1] * xv(i - P + 1) + cS[i - P] * xv(i - P) +
+                 cSE[i - P - 1] * xv(i - P - 1);
+            t[i] = b[i] - s;
+        });
+        __syncthreads();
+    }
+
+    // Up the V-cycle at coarse level l: x += P x_{l+1}, then one damped-Jacobi step into t.
+    __device__ __forceinline__ void smooth_up(int l) {
+        const Lvl L = lvl(l);
+        T *x = L.x, *t = L.t;
+        const T *b = L.b, *iv = L.iv;
+        prolong_add(l, x, LV<T>(l + 1, l + 1 == nlev - 1 ? LV_X : LV_T));
+        __syncthreads();
+        mark(PH_L_UP + (l < 3 ? l : 3) - 1);
+        for_cells(l, [&](int, int, int i) {
+            const T ivi = iv[i];
+            if (ivi != T(0)) t[i] = x[i] + ivi * (b[i] - applyc(L, x, i));
+        });
+        __syncthreads();
     }
 
     // ---- preconditioned CG on the T operator -------------------------------
@@ -968,12 +1046,11 @@ struct Win {
         int it = 0;
         while (it < maxit) {
             double pq = 0.0;
-            for (int k = threadIdx.x; k < nu; k += NT) {
-                const int i = ul[k];
-                const T qi = apply0(gT, p, i);
-                q[i] = qi;
-                pq += static_cast<double>(p[i]) * static_cast<double>(qi);
-            }
+            unknowns2([&](int i) { return TPair{apply0(gT, p, i), p[i]}; },
+                      [&](int i, const TPair &v) {
+                          q[i] = v.a;
+                          pq += static_cast<double>(v.b) * static_cast<double>(v.a);
+                      });
             pq = red.sum(pq);
             ++it;
             if (!(pq > 0.0) || !isfinite(pq)) {
@@ -1041,31 +1118,37 @@ struct Win {
         T *r = A<T>(AR_R);
         const bool series = a.series;
         double rr = 0.0, bb = 0.0;
-        for (int k = threadIdx.x; k < nu; k += NT) {
-            const int i = ul[k];
-            const double bi = b64[i];
-            double ri = bi;
-            if (!first) {
-                const double gi = g64[i], xi = x64[i];
-                double ao = 0.0, ad = 0.0;
+        (void)ul;
+        unknowns2(
+            [&](int i) {
+                const double bi = b64[i];
+                double ri = bi;
+                if (!first) {
+                    // every neighbour is read (padded box: finite values everywhere) and weighted 0 when it is no
+                    // node, so that all loads can be in flight together
+                    const double gi = g64[i], xi = x64[i];
+                    double ao = 0.0, ad = 0.0;
 #pragma unroll
-                for (int dd = 0; dd < ND; ++dd) {
-                    const int n = i + noff(dd);
-                    if (!(mask[n] & M_PRESENT)) continue;
-                    const double gn = g64[n];
-                    const double wv = series ? 2.0 / (1.0 / gi + 1.0 / gn) : gi + gn;
-                    if (NB::diag(dd))
-                        ad += wv * (xi - x64[n]);
-                    else
-                        ao += wv * (xi - x64[n]);
+                    for (int dd = 0; dd < ND; ++dd) {
+                        const int n = i + noff(dd);
+                        const bool on = (mask[n] & M_PRESENT) != 0;
+                        const double gn = g64[n], xn = x64[n];
+                        const double wv = on ? (series ? 2.0 / (1.0 / gi + 1.0 / gn) : gi + gn) : 0.0;
+                        if (NB::diag(dd))
+                            ad += wv * (xi - xn);
+                        else
+                            ao += wv * (xi - xn);
+                    }
+                    const double ax = series ? ao + ad * (1.0 / kSqrt2) : ao * 0.5 + ad * kInvTwoSqrt2;
+                    ri = bi - (ax + kShift * xi);
                 }
-                const double ax = series ? ao + ad * (1.0 / kSqrt2) : ao * 0.5 + ad * kInvTwoSqrt2;
-                ri = bi - (ax + kShift * xi);
-            }
-            r[i] = static_cast<T>(ri);
-            rr += ri * ri;
-            bb += bi * bi;
-        }
+                return DPair{ri, bi};
+            },
+            [&](int i, const DPair &v) {
+                r[i] = static_cast<T>(v.a);
+                rr += v.a * v.a;
+                bb += v.b * v.b;
+            });
         red.sum2(rr, bb);
         *rr_out = rr;
         *bb_out = bb;

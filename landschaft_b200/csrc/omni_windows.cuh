@@ -20,11 +20,13 @@ __global__ void __launch_bounds__(NT, 1) k_windows(const KArgs a) {
     __shared__ int scan_buf[64];
     __shared__ int lvh[kMaxLevels], lvw[kMaxLevels];
     __shared__ float lvinv[kMaxLevels];
+    __shared__ uint32_t lvoff[(kMaxLevels - 1) * LV_COUNT];
+    for (int k = threadIdx.x; k < (kMaxLevels - 1) * LV_COUNT; k += NT) lvoff[k] = a.lay.off[AR_LEVEL + k];
     __shared__ short cidx[kNcMax];
     __shared__ int item_s;
     char *gm = a.gscratch + static_cast<size_t>(blockIdx.x) * a.lay.gmem_bytes;
     Reducer<NT> red{red_buf, 0};
-    Win<NT, T, FOUR, MG, REFINE, HOT> win(a, smem, gm, red, scan_buf, lvh, lvw, lvinv, cidx);
+    Win<NT, T, FOUR, MG, REFINE, HOT> win(a, smem, gm, red, scan_buf, lvh, lvw, lvinv, lvoff, cidx);
 #ifdef LSB_PHASE_TIMERS
     __shared__ unsigned long long tacc[PH_COUNT + 1];
     if (threadIdx.x <= PH_COUNT) tacc[threadIdx.x] = threadIdx.x == PH_COUNT ? clock64() : 0ull;
