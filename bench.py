@@ -10,7 +10,8 @@ and scattered).
   scaling, no collective on the data path).
 * ``e2e``: the same metric through the drop-in ``landschaft_b200.omniscape(numpy, ...)`` call: host rasters
   in, host maps out, the copies inside the timed region.
-* ``fp64``: the plain FP64 Jacobi-PCG GPU path on the same workload; ``fp32_over_fp64`` their ratio.
+* ``fp64``: the plain FP64 Jacobi-PCG GPU path on the same workload; ``fp32_over_fp64`` their ratio.  The FP32
+  solve's preconditioner and threads per window are the autotuner's choice on a sample of the map's windows.
 * ``max_rel_err``: max relative error of the cumulative current over the cells above 1e-12 of the maximum,
   against the reference's own driver (oracle/_ref, FP64 direct solves) on the whole map, for both GPU solvers;
   also FP32 against FP64.
@@ -282,6 +283,9 @@ def main():
         d.close()
         return
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # 256 MiB > 126 MB L2
+    # the autotuner picks the FP32 solve's preconditioner and threads per window on a sample of the windows
+    # (outside the timed region); p32 leaves both on auto
+    tune = lsb.autotune(r, s, kw["radius"], buffer=kw["buffer"], block_size=kw["block_size"])
     # correctness and counts (outside the timed region)
     out32, stats32 = lsb_om.run_device(rt, st, p32)
     c32 = out32["current"].cpu().numpy()
@@ -348,7 +352,9 @@ def main():
                 "data": "synthetic (seeded Gaussian random field per rank; no dataset is published for this path)",
                 "config": {**WORKLOAD, "windows_per_rank": n_windows, "parallelism": f"{world} independent rasters",
                            "l2": "flushed between timed steps (256 MiB write)", "tol": 1e-12,
-                           "preconditioner": "multigrid V(1,1)"},
+                           "autotuned": {"preconditioner": tune["preconditioner"],
+                                         "threads_per_window": tune["threads_per_window"],
+                                         "sample_windows": tune["sample_windows"], "window_ms": tune["window_ms"]}},
                 "e2e": {"value": e2e, "unit": "windows/s", "h2d_bytes_per_step": int(r.nbytes + s.nbytes),
                         "d2h_bytes_per_step": int(r.nbytes)},
                 "fp64": {"value": fp64_value, "unit": "windows/s", "preconditioner": "jacobi",

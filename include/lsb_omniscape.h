@@ -180,6 +180,19 @@ int64_t lsb_last_launch_count(void);
  * return stats: their device time goes to stats->window_ms (profiling aid; 0 = off, the default). */
 void lsb_time_window_kernels(int32_t on);
 
+/* Tuning table (no counterpart in the reference): the preconditioner and threads per window that calls with
+ * preconditioner = LSB_PC_AUTO or threads_per_window = 0 use for windows window_width = 2 (radius + buffer) + 1
+ * cells wide, with these neighbours, edge weights and precision.  Entries come from an autotuning run
+ * (landschaft_b200.autotune) or a saved table; without one the built-in rule applies (FP64: Jacobi, FP32 +
+ * refinement: multigrid; 256 threads up to 1200 padded cells, else 512).  Process-wide and thread-safe.
+ * lsb_tune_set returns LSB_OK or LSB_ERR_ARGUMENT; lsb_tune_get returns 1 and fills the outputs when an entry
+ * exists, else 0. */
+int lsb_tune_set(int32_t window_width, int32_t four_neighbors, int32_t edge_weights, int32_t precision,
+                 int32_t preconditioner, int32_t threads_per_window);
+int lsb_tune_get(int32_t window_width, int32_t four_neighbors, int32_t edge_weights, int32_t precision,
+                 int32_t *preconditioner, int32_t *threads_per_window);
+void lsb_tune_clear(void);
+
 /* Library version string. */
 const char *lsb_version(void);
 

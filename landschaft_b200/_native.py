@@ -20,7 +20,8 @@ EDGE_AVERAGE, EDGE_SERIES = 0, 1
 # Every symbol the header declares (the CPU test checks the library exports them).
 EXPORTS = ("lsb_params_default", "lsb_omniscape_workspace_size", "lsb_omniscape", "lsb_omniscape_correction",
            "lsb_omniscape_grad", "lsb_omniscape_grad_workspace_size", "lsb_last_launch_count",
-           "lsb_time_window_kernels", "lsb_version", "lsb_omniscape_noalloc")
+           "lsb_time_window_kernels", "lsb_version", "lsb_omniscape_noalloc", "lsb_tune_set", "lsb_tune_get",
+           "lsb_tune_clear")
 
 
 class Condition(C.Structure):
@@ -94,6 +95,13 @@ def load():
         lib.lsb_omniscape_noalloc.restype = C.c_int
         lib.lsb_version.argtypes = []
         lib.lsb_version.restype = C.c_char_p
+        i32 = C.c_int32
+        lib.lsb_tune_set.argtypes = [i32] * 6
+        lib.lsb_tune_set.restype = C.c_int
+        lib.lsb_tune_get.argtypes = [i32] * 4 + [C.POINTER(i32), C.POINTER(i32)]
+        lib.lsb_tune_get.restype = C.c_int
+        lib.lsb_tune_clear.argtypes = []
+        lib.lsb_tune_clear.restype = None
         _lib = lib
         return lib
 

@@ -8,10 +8,12 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -115,11 +117,40 @@ int make_geom(int64_t nx, int64_t ny, const lsb_omni_params *p, Geom *g, char *e
 // ---------------------------------------------------------------------------
 struct Variant {
     int nt;       // threads per CTA
+    int pc;       // preconditioner (resolved)
     bool dbl;     // inner solve in double
     bool mg;      // multigrid compiled in
     bool refine;  // FP64 refinement around the inner solve
     bool four;
 };
+
+// ---------------------------------------------------------------------------
+// Tuning table: choices for parameters left on auto, per window shape and
+// arithmetic (filled by lsb_tune_set, e.g. from an autotuning run).
+// ---------------------------------------------------------------------------
+struct TuneKey {
+    int W, four, edge, prec;
+    bool operator<(const TuneKey &o) const {
+        if (W != o.W) return W < o.W;
+        if (four != o.four) return four < o.four;
+        if (edge != o.edge) return edge < o.edge;
+        return prec < o.prec;
+    }
+};
+struct TuneVal {
+    int pc, nt;
+};
+std::mutex g_tune_mutex;
+std::map<TuneKey, TuneVal> g_tune;
+std::atomic<uint64_t> g_tune_generation{0};  // part of the graph key: a new choice is a new launch sequence
+
+bool tune_lookup(const lsb_omni_params *p, int W, TuneVal *out) {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tune.find(TuneKey{W, p->four_neighbors != 0, p->edge_weights, p->precision});
+    if (it == g_tune.end()) return false;
+    *out = it->second;
+    return true;
+}
 
 Variant choose_variant(const lsb_omni_params *p, const Geom &g) {
     Variant v;
@@ -127,21 +158,21 @@ Variant choose_variant(const lsb_omni_params *p, const Geom &g) {
     v.dbl = p->precision == LSB_PREC_FP64;
     v.refine = !v.dbl;
     int pc = p->preconditioner;
-    if (pc == LSB_PC_AUTO) pc = v.dbl ? LSB_PC_JACOBI : LSB_PC_MG;
-    v.mg = pc == LSB_PC_MG;
     int nt = p->threads_per_window;
+    TuneVal tv;
+    if ((pc == LSB_PC_AUTO || (nt != 256 && nt != 512)) && tune_lookup(p, g.W, &tv)) {
+        if (pc == LSB_PC_AUTO) pc = tv.pc;
+        if (nt != 256 && nt != 512) nt = tv.nt;
+    }
+    if (pc == LSB_PC_AUTO) pc = v.dbl ? LSB_PC_JACOBI : LSB_PC_MG;
+    v.pc = pc;
+    v.mg = pc == LSB_PC_MG;
     if (nt != 256 && nt != 512) {
         const int np = (g.W + 2) * (g.W + 2);
         nt = np <= 1200 ? 256 : 512;
     }
     v.nt = nt;
     return v;
-}
-
-int resolved_pc(const lsb_omni_params *p) {
-    int pc = p->preconditioner;
-    if (pc == LSB_PC_AUTO) pc = p->precision == LSB_PREC_FP64 ? LSB_PC_JACOBI : LSB_PC_MG;
-    return pc;
 }
 
 constexpr size_t kStaticSmem = 2048;  // the window kernel's static shared memory, with room to spare
@@ -311,13 +342,13 @@ int make_plan(int64_t nx, int64_t ny, const lsb_omni_params *p, Plan *pl, char *
     return LSB_OK;
 }
 
-SolveParams solve_params(const lsb_omni_params *p) {
+SolveParams solve_params(const lsb_omni_params *p, int pc) {
     SolveParams sp;
     sp.tol = p->tol > 0 ? p->tol : 1e-12;
     sp.inner_tol = p->precision == LSB_PREC_FP64 ? sp.tol : 1e-4;
     sp.max_iter = p->max_iter > 0 ? p->max_iter : 20000;
     sp.max_outer = 12;
-    sp.pc = resolved_pc(p);
+    sp.pc = pc;
     sp.omega = 0.7f;
     return sp;
 }
@@ -332,6 +363,7 @@ struct GraphKey {
     size_t ws_bytes;
     void *stream;
     int dev;
+    uint64_t tune_generation;
     bool operator==(const GraphKey &o) const { return std::memcmp(this, &o, sizeof *this) == 0; }
 };
 struct GraphEntry {
@@ -408,7 +440,7 @@ int enqueue(const Plan &pl, const double *res, const double *src, const lsb_omni
     a.timers = reinterpret_cast<unsigned long long *>(ws + pl.o_timers);
     LSB_CK(cudaMemsetAsync(a.timers, 0, sizeof(unsigned long long) * 30, s));
 #endif
-    a.sp = solve_params(p);
+    a.sp = solve_params(p, pl.v.pc);
     if (g.conditions && g.NL > 0) {
         k_block_cond<<<static_cast<int>((g.NL + 127) / 128), 128, 0, s>>>(
             a, reinterpret_cast<double *>(ws + pl.o_condv), errf);
@@ -534,6 +566,7 @@ int lsb_omniscape(const double *resistance, const double *source, int64_t nx, in
         key.stream = stream;
         key.dev = 0;
         cudaGetDevice(&key.dev);
+        key.tune_generation = g_tune_generation.load();
         std::lock_guard<std::mutex> lock(g_graph_mutex);
         cudaGraphExec_t exec = nullptr;
         int64_t launches = 0;
@@ -620,7 +653,7 @@ int lsb_omniscape(const double *resistance, const double *source, int64_t nx, in
         stats->refine_max = ds.refine_max;
         stats->batches = pl.nbatches;
         stats->threads_per_window = pl.v.nt;
-        stats->preconditioner = resolved_pc(p);
+        stats->preconditioner = pl.v.pc;
         stats->worst_residual = ds.worst_residual;
         stats->unknown_iters = ds.unknown_iters;
         if (hdr[1]) {
@@ -767,7 +800,7 @@ int lsb_omniscape_correction(int32_t radius, int32_t buffer, int32_t block_size,
     c.queue = queue;
     c.gscratch = reinterpret_cast<char *>(queue) + align_up(8);
     c.lay = pl.lay;
-    c.sp = solve_params(&p);
+    c.sp = solve_params(&p, pl.v.pc);
     LSB_CK(cudaMemsetAsync(queue, 0, 4, s));
     pl.kern<<<2, pl.v.nt, pl.lay.smem_bytes, s>>>(c);
     k_corr_ratio<<<1, 1024, 0, s>>>(c.cur_win, c.stat, g.W, g.bs, corr);
@@ -860,7 +893,7 @@ int lsb_omniscape_grad(const double *resistance, const double *source, const dou
     a.lat_amps = amps;
     a.gscratch = ws + pl.o_gs;
     a.lay = pl.lay;
-    a.sp = solve_params(p);
+    a.sp = solve_params(p, pl.v.pc);
     a.mode = 2;
     a.weight = weight;
     a.Jw = Jw;
@@ -906,7 +939,7 @@ int lsb_omniscape_grad(const double *resistance, const double *source, const dou
         stats->refine_max = ds.refine_max;
         stats->batches = pl.nbatches;
         stats->threads_per_window = pl.v.nt;
-        stats->preconditioner = resolved_pc(p);
+        stats->preconditioner = pl.v.pc;
         stats->worst_residual = ds.worst_residual;
         stats->unknown_iters = ds.unknown_iters;
         if (ds.n_failed > 0) {
@@ -921,6 +954,38 @@ int lsb_omniscape_grad(const double *resistance, const double *source, const dou
 int64_t lsb_last_launch_count(void) { return g_launches; }
 
 void lsb_time_window_kernels(int32_t on) { g_time_windows = on != 0; }
+
+int lsb_tune_set(int32_t window_width, int32_t four_neighbors, int32_t edge_weights, int32_t precision,
+                 int32_t preconditioner, int32_t threads_per_window) {
+    if (window_width < 1 || (preconditioner != LSB_PC_JACOBI && preconditioner != LSB_PC_MG) ||
+        (threads_per_window != 256 && threads_per_window != 512))
+        return LSB_ERR_ARGUMENT;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        g_tune[TuneKey{window_width, four_neighbors != 0, edge_weights, precision}] =
+            TuneVal{preconditioner, threads_per_window};
+    }
+    ++g_tune_generation;
+    return LSB_OK;
+}
+
+int lsb_tune_get(int32_t window_width, int32_t four_neighbors, int32_t edge_weights, int32_t precision,
+                 int32_t *preconditioner, int32_t *threads_per_window) {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tune.find(TuneKey{window_width, four_neighbors != 0, edge_weights, precision});
+    if (it == g_tune.end()) return 0;
+    if (preconditioner) *preconditioner = it->second.pc;
+    if (threads_per_window) *threads_per_window = it->second.nt;
+    return 1;
+}
+
+void lsb_tune_clear(void) {
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        g_tune.clear();
+    }
+    ++g_tune_generation;
+}
 
 const char *lsb_version(void) { return "landschaft_b200 0.1 (sm_100a)"; }
 

@@ -152,3 +152,28 @@ def test_synthetic_workloads():
     assert 0.05 <= p.mean() < 0.08
     # deterministic
     np.testing.assert_array_equal(synthetic.omni_grf(64, 3)[0], synthetic.omni_grf(64, 3)[0])
+
+
+def test_tuning_table_set_get_clear_and_file(tmp_path):
+    # the table is host state of the library: no device needed
+    lib = N.load()
+    lsb.clear_tuning()
+    pc, nt = C.c_int32(-1), C.c_int32(-1)
+    assert lib.lsb_tune_get(65, 0, 0, N.PREC_FP32_REFINE, C.byref(pc), C.byref(nt)) == 0
+    assert lib.lsb_tune_set(65, 0, 0, N.PREC_FP32_REFINE, 3, 256) != 0  # no such preconditioner
+    assert lib.lsb_tune_set(65, 0, 0, N.PREC_FP32_REFINE, 1, 384) != 0  # no such block size
+    entry = {"window": 65, "four_neighbors": False, "edge_weights": "average", "solver": "fp32-refine",
+             "preconditioner": "jacobi", "threads_per_window": 256}
+    from landschaft_b200 import tune
+    tune._install(entry)
+    assert lib.lsb_tune_get(65, 0, 0, N.PREC_FP32_REFINE, C.byref(pc), C.byref(nt)) == 1
+    assert (pc.value, nt.value) == (1, 256)
+    assert lib.lsb_tune_get(65, 1, 0, N.PREC_FP32_REFINE, C.byref(pc), C.byref(nt)) == 0  # other neighbourhood
+    path = tmp_path / "tuning.json"
+    lsb.save_tuning(path)
+    lsb.clear_tuning()
+    assert lib.lsb_tune_get(65, 0, 0, N.PREC_FP32_REFINE, C.byref(pc), C.byref(nt)) == 0
+    assert lsb.load_tuning(path) == 1
+    assert lib.lsb_tune_get(65, 0, 0, N.PREC_FP32_REFINE, C.byref(pc), C.byref(nt)) == 1
+    assert lsb.tuning_table()[0]["preconditioner"] == "jacobi"
+    lsb.clear_tuning()
