@@ -116,6 +116,7 @@ __host__ __device__ constexpr bool hot_array(int k) {
 // compile to 32-bit shared addressing (else each pointer is chosen at run time and addressed generically).
 template <int NT, typename T, bool FOUR, bool MG, bool REFINE, bool HOT>
 struct Win {
+    static_assert(REFINE || sizeof(T) == 8, "an FP32 inner solve needs the FP64 refinement");
     using NB = Nb<FOUR>;
     static constexpr int ND = NB::ND, LOWER = NB::LOWER;
 
@@ -1011,8 +1012,9 @@ struct Win {
     }
 
     // ---- preconditioned CG on the T operator -------------------------------
-    // Solves A d = r0 (r holds r0 on entry, the residual on exit) to relative
-    // residual rtol or for at most maxit iterations.  d must be 0 on entry.
+    // Adds to d the CG solution of A e = r0 (r holds r0 = b - A d on entry, the
+    // recursively updated residual on exit), to relative residual rtol or for at
+    // most maxit iterations.
     // Returns the iterations; *ok = false on breakdown.
     __device__ __forceinline__ int pcg(T *d, T *r, double rtol, int maxit, bool use_mg, bool *ok) {
         const uint16_t *ul = A<uint16_t>(AR_ULIST);
@@ -1167,24 +1169,40 @@ struct Win {
         int iters = 0, outer = 0, status = 1;
         double rel = 0.0;
         if (!REFINE) {
-            // one CG run on the T = double operator, straight to the tolerance
-            T *d = sizeof(T) == 8 ? reinterpret_cast<T *>(x64) : A<T>(AR_D);
+            // CG on the double operator, from the current iterate: the stopping test of CG reads the recursively
+            // updated residual, which drifts from b - A x on ill-conditioned windows, so every run ends with the
+            // true FP64 residual, and CG restarts from it (residual replacement) until that meets the tolerance
+            T *d = reinterpret_cast<T *>(x64);
             T *r = A<T>(AR_R);
             double rr, bb;
             residual64(&rr, &bb, true);  // r = b (barrier)
+            double prev = CUDART_INF;
             bool ok = true;
-            iters = pcg(d, r, a.sp.tol, a.sp.max_iter, want_mg, &ok);
-            outer = 1;
-            __syncthreads();
-            if (sizeof(T) != 8) {
-                for (int k = threadIdx.x; k < nu; k += NT) x64[ul[k]] = static_cast<double>(d[ul[k]]);
+            while (true) {
+                rel = bb > 0 ? sqrt(rr / bb) : 0.0;
+                if (!isfinite(rel)) {
+                    status = 3;
+                    break;
+                }
+                if (rel <= a.sp.tol) break;
+                if (!ok) {
+                    status = 3;
+                    break;
+                }
+                // a restart that gained less than half an order has met the FP64 rounding floor: accepted
+                // within kFloor x tol, as in the refinement below
+                constexpr double kFloor = 100.0;
+                if (outer >= a.sp.max_outer || iters >= a.sp.max_iter || rel > 0.5 * prev) {
+                    status = rel <= kFloor * a.sp.tol ? 1 : 2;
+                    break;
+                }
+                prev = rel;
+                const int budget = a.sp.max_iter - iters;
+                iters += pcg(d, r, fmin(0.5, a.sp.tol / rel), budget < 1 ? 1 : budget, want_mg, &ok);
+                ++outer;
                 __syncthreads();
+                residual64(&rr, &bb, false);  // the true residual, into r
             }
-            double rr2, bb2;
-            residual64(&rr2, &bb2, false);
-            rel = bb2 > 0 ? sqrt(rr2 / bb2) : 0.0;
-            if (!ok || !isfinite(rel)) status = 3;
-            else if (iters >= a.sp.max_iter && rel > a.sp.tol) status = 2;
         } else {
             T *d = A<T>(AR_D), *r = A<T>(AR_R);
             bool use_mg = want_mg;

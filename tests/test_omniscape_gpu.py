@@ -154,6 +154,24 @@ def test_config_128_full(lsb):
         check_against(ds, ref)
 
 
+def test_config_4096_radius64_crop(lsb):
+    # the 4096 x 4096, radius 64, block 5 workload (129-cell windows, solver arrays in global scratch): a
+    # 256 x 256 crop, every window, against the reference's own driver, at the 1e-6 bar of the FP32 solve
+    from landschaft_b200 import synthetic
+    r, s, kw = synthetic.omni_4096()
+    r = np.ascontiguousarray(r[3500:3756, 3000:3256])
+    s = np.ascontiguousarray(s[3500:3756, 3000:3256])
+    impl = "ref" if oracle.REF_AVAILABLE else "port"
+    ref = oracle.core_omniscape(r, s, kw["radius"], 0, kw["block_size"], False, False, True, False, impl=impl)
+    ds, stats = lsb.omniscape(r, kw["radius"], source=s, block_size=kw["block_size"], mask_nodata=False,
+                              return_stats=True)
+    assert ds.attrs["n_targets"] == ref["n_targets"] >= 500
+    assert stats["n_failed"] == 0
+    cur = _values(ds, "cum_currmap")
+    assert max_rel(cur, ref["current"]) <= 1e-6
+    np.testing.assert_array_equal(cur == 0, ref["current"] == 0)
+
+
 def test_deterministic_and_graph_replay(lsb):
     r = _map(3, (50, 60))
     s = np.where(np.isnan(r), 0, 1 / np.nan_to_num(r, nan=1))
