@@ -349,7 +349,7 @@ SolveParams solve_params(const lsb_omni_params *p, int pc) {
     sp.max_iter = p->max_iter > 0 ? p->max_iter : 20000;
     sp.max_outer = 12;
     sp.pc = pc;
-    sp.omega = 0.7f;
+    sp.omega = 0.9f;
     return sp;
 }
 

@@ -281,27 +281,59 @@ struct Win {
         const bool has = mask[ground] & M_CAND;
         __syncthreads();
         if (!has) return false;
-        if (threadIdx.x == 0) mask[ground] = M_CAND | M_PRESENT;
+        // Bit rows over the padded box (bit px of word px / 32 of row py), held in the CG vector P until the
+        // assembly clears it: candidates cb and reached cells pb, pb starting at the ground.  A sweep sets in
+        // every word the candidates next to a reached cell (word-wise dilation, carries from the neighbouring
+        // words); it is monotone, so words written during a sweep may be read old or new, and the sweeps end
+        // when one changes nothing: pb is then the ground's component.
+        const int P = G.P, words = (P + 31) >> 5, nrow = G.h + 2, ntask = nrow * words;
+        const float invwd = 1.0f / static_cast<float>(words);  // (k + 0.5) / words in float: exact row, k < 2^16
+        uint32_t *cb = reinterpret_cast<uint32_t *>(A<T>(AR_P)), *pb = cb + ntask;
+        const int gpy = G.gy + 1, gpx = G.gx + 1;
+        const int lane = threadIdx.x & 31;
+        for (int k = threadIdx.x >> 5; k < ntask; k += NT / 32) {
+            const int py = static_cast<int>((static_cast<float>(k) + 0.5f) * invwd), w = k - py * words;
+            const int px = 32 * w + lane;
+            const bool c = px < P && (mask[py * P + px] & M_CAND) != 0;
+            const uint32_t bits = __ballot_sync(0xffffffffu, c);
+            if (lane == 0) {
+                cb[k] = bits;
+                pb[k] = (py == gpy && w == (gpx >> 5)) ? (1u << (gpx & 31)) : 0u;
+            }
+        }
         __syncthreads();
-        int sweep = 0;
+        volatile uint32_t *vp = pb;
         while (true) {
             int changed = 0;
-            const bool fwd = (sweep & 1) == 0;
-            const int start = fwd ? static_cast<int>(threadIdx.x) : G.NP - 1 - static_cast<int>(threadIdx.x);
-            for (int i = start; fwd ? i < G.NP : i >= 0; i += fwd ? NT : -NT) {
-                const uint8_t m = mask[i];
-                if ((m & (M_CAND | M_PRESENT)) != M_CAND) continue;
-                bool any = false;
-#pragma unroll
-                for (int d = 0; d < ND; ++d) any |= (static_cast<volatile uint8_t *>(mask)[i + noff(d)] & M_PRESENT) != 0;
-                if (any) {
-                    mask[i] = m | M_PRESENT;
+            for (int k = threadIdx.x; k < ntask; k += NT) {
+                const uint32_t c = cb[k];
+                if (!c) continue;  // padding rows hold no candidate: rows py - 1 and py + 1 exist below
+                const int py = static_cast<int>((static_cast<float>(k) + 0.5f) * invwd), w = k - py * words;
+                const uint32_t mid = vp[k];
+                const bool hl = w > 0, hr = w + 1 < words;
+                uint32_t nb;
+                if (FOUR) {
+                    const uint32_t l = hl ? vp[k - 1] : 0u, r = hr ? vp[k + 1] : 0u;
+                    nb = vp[k - words] | vp[k + words] | (mid << 1) | (l >> 31) | (mid >> 1) | (r << 31);
+                } else {
+                    const uint32_t v = vp[k - words] | mid | vp[k + words];
+                    const uint32_t vl = hl ? (vp[k - words - 1] | vp[k - 1] | vp[k + words - 1]) : 0u;
+                    const uint32_t vr = hr ? (vp[k - words + 1] | vp[k + 1] | vp[k + words + 1]) : 0u;
+                    nb = v | (v << 1) | (vl >> 31) | (v >> 1) | (vr << 31);
+                }
+                const uint32_t nw = c & (mid | nb);
+                if (nw != mid) {
+                    vp[k] = nw;
                     changed = 1;
                 }
             }
-            ++sweep;
             if (!__syncthreads_or(changed)) break;
         }
+        for (int i = threadIdx.x; i < G.NP; i += NT) {
+            const int py = row0(i), px = i - py * P;
+            if ((pb[py * words + (px >> 5)] >> (px & 31)) & 1u) mask[i] |= M_PRESENT;
+        }
+        __syncthreads();
         return true;
     }
 
