@@ -175,7 +175,11 @@ Variant choose_variant(const lsb_omni_params *p, const Geom &g) {
     return v;
 }
 
+#ifdef LSB_PHASE_TIMERS
+constexpr size_t kStaticSmem = 3072;  // the window kernel's static shared memory with the phase counters
+#else
 constexpr size_t kStaticSmem = 2048;  // the window kernel's static shared memory, with room to spare
+#endif
 
 ArenaLayout make_layout(const Variant &v, int W, size_t smem_budget, bool grad) {
     ArenaLayout L;
@@ -205,7 +209,7 @@ ArenaLayout make_layout(const Variant &v, int W, size_t smem_budget, bool grad) 
             const size_t npl = static_cast<size_t>(h + 2) * (w + 2);
             for (int k = 0; k < LV_COUNT; ++k) items.push_back({AR_LEVEL + (l - 1) * LV_COUNT + k, npl * ts});
         }
-        items.push_back({AR_DENSE, static_cast<size_t>(kNcMax) * kNcMax * 8});
+        items.push_back({AR_DENSE, static_cast<size_t>(kNcMax) * (kNcMax + 2) * 8});  // + pivot column, diagonal
     }
     items.push_back({AR_MASK, np});
     if (!has_d) items.push_back({AR_X64, np * 8});  // the solution is the iterate: keep it close
@@ -629,10 +633,10 @@ int lsb_omniscape(const double *resistance, const double *source, int64_t nx, in
             unsigned long long tm[PH_COUNT];
             LSB_CK(cudaMemcpy(tm, ws + pl.o_timers, sizeof tm, cudaMemcpyDeviceToHost));
             static const char *names[PH_COUNT] = {"load", "flood", "mark", "assemble", "mg_setup", "resid64", "cg",
-                                                  "vcycle", "currents", "other", "v_pre0", "v_restrict1", "v_down",
-                                                  "v_coarsest", "v_up", "v_prolong0", "v_post0",
-                                                  "ds1", "ds2", "ds3", "dr1", "dr2", "dr3", "up1", "up2", "up3",
-                                                  "us1", "us2", "us3"};
+                                                  "vcycle", "currents", "other", "v_pre0", "v_restrict1",
+                                                  "v_coarsest", "v_prolong0", "v_post0", "s_weights", "s_level1",
+                                                  "s_coarser", "s_dense", "ds1", "ds2+", "dr1", "dr2+", "up1",
+                                                  "up2+", "us1", "us2+"};
             double tot = 0;
             for (int k = 0; k < PH_COUNT; ++k) tot += static_cast<double>(tm[k]);
             fprintf(stderr, "[phases] windows=%d cycles/window:", hdr[0]);

@@ -48,10 +48,12 @@ struct KArgs {
 
 // Phases of a window solve, for the cycle counters of profiling builds.
 enum Phase : int { PH_LOAD = 0, PH_FLOOD, PH_MARK, PH_ASSEMBLE, PH_MG_SETUP, PH_RESID, PH_CG, PH_VCYCLE, PH_CURRENTS,
-                   PH_OTHER, PH_V_PRE0, PH_V_RESTRICT1, PH_V_DOWN, PH_V_COARSEST, PH_V_UP, PH_V_PROLONG0, PH_V_POST0,
-                   // levels 1-3 (deeper levels count as 3): down smoothing, restriction; up prolongation, smoothing
-                   PH_L_DS, PH_L_DR = PH_L_DS + 3, PH_L_UP = PH_L_DR + 3, PH_L_US = PH_L_UP + 3,
-                   PH_COUNT = PH_L_US + 3 };
+                   PH_OTHER, PH_V_PRE0, PH_V_RESTRICT1, PH_V_COARSEST, PH_V_PROLONG0, PH_V_POST0,
+                   // multigrid set-up: level-0 weights, level-1 Galerkin product, coarser products, coarsest inverse
+                   PH_S_W, PH_S_L1, PH_S_LC, PH_S_DENSE,
+                   // levels 1 and 2 (deeper levels count as 2): down smoothing, restriction; up prolongation, smoothing
+                   PH_L_DS, PH_L_DR = PH_L_DS + 2, PH_L_UP = PH_L_DR + 2, PH_L_US = PH_L_UP + 2,
+                   PH_COUNT = PH_L_US + 2 };
 static_assert(PH_COUNT <= 30, "two timer slots are calibration");
 
 template <typename X>
@@ -678,6 +680,7 @@ struct Win {
         }
         if (nlev > 1) weights0(true);  // ends with a barrier
         __syncthreads();
+        mark(PH_S_W);
         for (int l = 1; l < nlev; ++l) {
             const int hf = lvh[l - 1], wf = lvw[l - 1];
             const int hc = lvh[l], wc = lvw[l], NPc = (hc + 2) * (wc + 2);
@@ -721,13 +724,15 @@ struct Win {
             });
             __syncthreads();
             if (l == 1) weights0(false);
+            mark(l == 1 ? PH_S_L1 : PH_S_LC);
         }
         dense_setup();
+        mark(PH_S_DENSE);
     }
 
-    // Pseudo-inverse of the coarsest operator (at most kNcMax cells): Cholesky
-    // with skipped (near-zero) pivots, then one column of the inverse per lane.
-    // Also lists the coarsest cells' padded indices (cidx).
+    // Pseudo-inverse of the coarsest operator (at most kNcMax cells), full and
+    // symmetric in M (row stride kNcMax).  Also lists the coarsest cells' padded
+    // indices (cidx).
     __device__ __forceinline__ void dense_setup() {
         double *M = A<double>(AR_DENSE);
         const int l = nlev - 1;
@@ -754,63 +759,41 @@ struct Win {
             M[e] = val;
         }
         __syncthreads();
-        if (threadIdx.x < 32) {
-            const int lane = threadIdx.x;
-            // in-place lower Cholesky; skipped pivots get L = identity column
-            unsigned skip_bits = 0u;
-            const double od = lane < n ? M[lane * kNcMax + lane] : 0.0;  // original diagonal
-            for (int k = 0; k < n; ++k) {
-                const double piv = M[k * kNcMax + k];
-                const double odk = __shfl_sync(0xffffffffu, od, k);
-                // a Schur-complement pivot that vanished against the original diagonal: a
-                // dependent direction of the masked prolongation; left out of the inverse
-                const bool skip = !(piv > 1e-10 * odk);
-                if (skip) {
-                    skip_bits |= 1u << k;
-                    if (lane < n) M[lane * kNcMax + k] = lane == k ? 1.0 : 0.0;
-                    __syncwarp();
-                    continue;
-                }
-                const double lkk = sqrt(piv);
-                __syncwarp();
-                if (lane > k && lane < n) M[lane * kNcMax + k] /= lkk;
-                if (lane == k) M[k * kNcMax + k] = lkk;
-                __syncwarp();
-                if (lane > k && lane < n) {
-                    const double lik = M[lane * kNcMax + k];
-                    for (int j = k + 1; j <= lane; ++j) M[lane * kNcMax + j] -= lik * M[j * kNcMax + k];
-                }
-                __syncwarp();
+        // Symmetric sweep (Gauss-Jordan on a symmetric matrix), one pivot after another with every thread on the
+        // update: at step k the pivot is the Schur complement of the pivots swept before it, the value the
+        // Cholesky factorisation meets.  A pivot that vanished against the original diagonal (a dependent
+        // direction of the masked prolongation) is skipped.  After the last step the swept block holds minus the
+        // inverse of the non-skipped principal submatrix; skipped rows and columns become zero.
+        double *colk = M + kNcMax * kNcMax, *od = colk + kNcMax;
+        unsigned *skip = reinterpret_cast<unsigned *>(scan);
+        if (threadIdx.x < n) od[threadIdx.x] = M[threadIdx.x * kNcMax + threadIdx.x];
+        if (threadIdx.x == 0) *skip = 0u;
+        for (int k = 0; k < n; ++k) {
+            __syncthreads();  // the previous step's writes (and od, skip) visible
+            if (threadIdx.x < n) colk[threadIdx.x] = M[threadIdx.x * kNcMax + k];
+            if (threadIdx.x == 0 && !(M[k * kNcMax + k] > 1e-10 * od[k])) *skip |= 1u << k;
+            __syncthreads();
+            if ((*skip >> k) & 1u) continue;
+            const double inv = 1.0 / colk[k];
+            for (int e = threadIdx.x; e < n * n; e += NT) {
+                const int i = e / n, j = e - i * n;
+                double v;
+                if (i == k && j == k)
+                    v = -inv;
+                else if (i == k)
+                    v = colk[j] * inv;
+                else if (j == k)
+                    v = colk[i] * inv;
+                else
+                    v = M[i * kNcMax + j] - colk[i] * (colk[j] * inv);
+                M[i * kNcMax + j] = v;
             }
-            const unsigned sk = skip_bits;
-            // column `lane` of the inverse: L y = e_lane, then L^T x = y, skipped unknowns at 0
-            double col[kNcMax];
-            if (lane < n) {
-                for (int i = 0; i < n; ++i) col[i] = 0.0;
-                if (!((sk >> lane) & 1u)) col[lane] = 1.0;
-                for (int i = 0; i < n; ++i) {
-                    if ((sk >> i) & 1u) {
-                        col[i] = 0.0;
-                        continue;
-                    }
-                    double s = col[i];
-                    for (int k = 0; k < i; ++k) s -= M[i * kNcMax + k] * col[k];
-                    col[i] = s / M[i * kNcMax + i];
-                }
-                for (int i = n - 1; i >= 0; --i) {
-                    if ((sk >> i) & 1u) {
-                        col[i] = 0.0;
-                        continue;
-                    }
-                    double s = col[i];
-                    for (int k = i + 1; k < n; ++k) s -= M[k * kNcMax + i] * col[k];
-                    col[i] = s / M[i * kNcMax + i];
-                }
-            }
-            __syncwarp();
-            // column `lane` of the (symmetric) inverse, after every lane has read L: M holds the full inverse
-            if (lane < n)
-                for (int i = 0; i < n; ++i) M[i * kNcMax + lane] = col[i];
+        }
+        __syncthreads();
+        const unsigned sk = *skip;
+        for (int e = threadIdx.x; e < n * n; e += NT) {
+            const int i = e / n, j = e - i * n;
+            M[i * kNcMax + j] = (((sk >> i) | (sk >> j)) & 1u) ? 0.0 : -M[i * kNcMax + j];
         }
         __syncthreads();
     }
@@ -849,19 +832,17 @@ struct Win {
         mark(PH_V_RESTRICT1);
         for (int l = 1; l < nlev - 1; ++l) {
             smooth_down(l);
-            mark(PH_L_DS + (l < 3 ? l : 3) - 1);
+            mark(PH_L_DS + (l < 2 ? 0 : 1));
             restrict_to(l + 1, LV<T>(l, LV_T));
-            mark(PH_L_DR + (l < 3 ? l : 3) - 1);
+            mark(PH_L_DR + (l < 2 ? 0 : 1));
         }
-        mark(PH_V_DOWN);
         coarse_solve(nlev - 1, LV<T>(nlev - 1, LV_B), LV<T>(nlev - 1, LV_X));
         __syncthreads();
         mark(PH_V_COARSEST);
         for (int l = nlev - 2; l >= 1; --l) {
             smooth_up(l);
-            mark(PH_L_US + (l < 3 ? l : 3) - 1);
+            mark(PH_L_US + (l < 2 ? 0 : 1));
         }
-        mark(PH_V_UP);
         prolong_add(0, z, LV<T>(1, nlev - 1 == 1 ? LV_X : LV_T));
         __syncthreads();
         mark(PH_V_PROLONG0);
@@ -1035,7 +1016,7 @@ struct Win {
         const T *b = L.b, *iv = L.iv;
         prolong_add(l, x, LV<T>(l + 1, l + 1 == nlev - 1 ? LV_X : LV_T));
         __syncthreads();
-        mark(PH_L_UP + (l < 3 ? l : 3) - 1);
+        mark(PH_L_UP + (l < 2 ? 0 : 1));
         for_cells(l, [&](int, int, int i) {
             const T ivi = iv[i];
             if (ivi != T(0)) t[i] = x[i] + ivi * (b[i] - applyc(L, x, i));

@@ -34,12 +34,12 @@ __global__ void __launch_bounds__(NT, 1) k_windows(const KArgs a) {
     win.tacc = tacc;
     if (blockIdx.x == 0 && a.timers) {
         // calibration: 64 bare barriers, then 64 barrier-separated shared-memory round trips
-        __shared__ float cal[1024];
+        __shared__ float cal[64];  // small: the timers build must fit the layouts that fill shared memory
         unsigned long long t0 = clock64();
         for (int k = 0; k < 64; ++k) __syncthreads();
         unsigned long long t1 = clock64();
         for (int k = 0; k < 64; ++k) {
-            cal[threadIdx.x] = cal[(threadIdx.x + 1) % NT] + 1.0f;
+            if (threadIdx.x < 64) cal[threadIdx.x] = cal[(threadIdx.x + 1) & 63] + 1.0f;
             __syncthreads();
         }
         unsigned long long t2 = clock64();
