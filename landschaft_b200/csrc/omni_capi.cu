@@ -237,6 +237,14 @@ ArenaLayout make_layout(const Variant &v, int W, size_t smem_budget, bool grad) 
     L.hot = 1;
     for (const Item &it : items)
         if (hot_array(it.arr) && (L.off[it.arr] & 0x80000000u)) L.hot = 0;
+    // the node currents read the FP64 conductance and potentials at every neighbour: when those sit in global
+    // scratch, the span from the stencil conductances to the mask (solver vectors, levels, coarsest inverse: dead
+    // by then) holds copies of both if it is large enough
+    L.stage = kNoStage;
+    const bool g_global = (L.off[AR_G64] & 0x80000000u) || (L.off[AR_X64] & 0x80000000u);
+    if (L.hot && g_global && !(L.off[AR_MASK] & 0x80000000u) && L.off[AR_MASK] > L.off[AR_GT] &&
+        L.off[AR_MASK] - L.off[AR_GT] >= 2 * np * 8)
+        L.stage = L.off[AR_GT];
     return L;
 }
 

@@ -121,11 +121,14 @@ enum ArenaArray : int {
 };
 
 // Byte offsets of the arrays; bit 31 set: in global scratch, else shared.
+constexpr uint32_t kNoStage = 0xffffffffu;
+
 struct ArenaLayout {
     uint32_t off[AR_COUNT];
     uint32_t smem_bytes;
     uint32_t gmem_bytes;  // per CTA
     uint32_t hot;         // 1: every array but the FP64 window arrays is in shared memory
+    uint32_t stage;       // shared offset of 2 x (h+2)(w+2) doubles free during the node currents, or kNoStage
 };
 
 // Solver configuration for one launch.

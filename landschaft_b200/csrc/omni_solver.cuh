@@ -768,33 +768,40 @@ struct Win {
         unsigned *skip = reinterpret_cast<unsigned *>(scan);
         if (threadIdx.x < n) od[threadIdx.x] = M[threadIdx.x * kNcMax + threadIdx.x];
         if (threadIdx.x == 0) *skip = 0u;
+        const int jl = threadIdx.x & 31;  // column of this thread; rows by warp (n <= kNcMax <= 32)
         for (int k = 0; k < n; ++k) {
             __syncthreads();  // the previous step's writes (and od, skip) visible
             if (threadIdx.x < n) colk[threadIdx.x] = M[threadIdx.x * kNcMax + k];
-            if (threadIdx.x == 0 && !(M[k * kNcMax + k] > 1e-10 * od[k])) *skip |= 1u << k;
+            if (threadIdx.x == 0) {
+                const double piv = M[k * kNcMax + k];
+                if (!(piv > 1e-10 * od[k]))
+                    *skip |= 1u << k;
+                else
+                    od[k] = 1.0 / piv;  // the original diagonal of k is not read again
+            }
             __syncthreads();
             if ((*skip >> k) & 1u) continue;
-            const double inv = 1.0 / colk[k];
-            for (int e = threadIdx.x; e < n * n; e += NT) {
-                const int i = e / n, j = e - i * n;
-                double v;
-                if (i == k && j == k)
-                    v = -inv;
-                else if (i == k)
-                    v = colk[j] * inv;
-                else if (j == k)
-                    v = colk[i] * inv;
-                else
-                    v = M[i * kNcMax + j] - colk[i] * (colk[j] * inv);
-                M[i * kNcMax + j] = v;
+            const double inv = od[k];
+            if (jl < n) {
+                for (int i = threadIdx.x >> 5; i < n; i += NT / 32) {
+                    double v;
+                    if (i == k && jl == k)
+                        v = -inv;
+                    else if (i == k)
+                        v = colk[jl] * inv;
+                    else if (jl == k)
+                        v = colk[i] * inv;
+                    else
+                        v = M[i * kNcMax + jl] - colk[i] * (colk[jl] * inv);
+                    M[i * kNcMax + jl] = v;
+                }
             }
         }
         __syncthreads();
         const unsigned sk = *skip;
-        for (int e = threadIdx.x; e < n * n; e += NT) {
-            const int i = e / n, j = e - i * n;
-            M[i * kNcMax + j] = (((sk >> i) | (sk >> j)) & 1u) ? 0.0 : -M[i * kNcMax + j];
-        }
+        if (jl < n)
+            for (int i = threadIdx.x >> 5; i < n; i += NT / 32)
+                M[i * kNcMax + jl] = (((sk >> i) | (sk >> jl)) & 1u) ? 0.0 : -M[i * kNcMax + jl];
         __syncthreads();
     }
 
@@ -805,7 +812,9 @@ struct Win {
 
     // z = B r: one V(1,1) cycle, damped-Jacobi smoothing, exact coarsest.
     // r is level-0 (unknowns only); the result goes to AR_Q; AR_Z is scratch.
-    __device__ __forceinline__ void vcycle(const T *r) {
+    // Also adds this thread's terms of r.z and r.r to rz and rr (its unknowns in increasing order), and copies z
+    // to pcopy when given.
+    __device__ __forceinline__ void vcycle(const T *r, double &rz, double &rr, T *pcopy = nullptr) {
         const uint16_t *ul = A<uint16_t>(AR_ULIST);
         const T *gT = A<T>(AR_GT), *invd = A<T>(AR_INVD);
         T *z = A<T>(AR_Z), *q = A<T>(AR_Q);
@@ -813,6 +822,13 @@ struct Win {
             // the window is its own coarsest level
             coarse_solve(0, r, q);
             __syncthreads();
+            for (int k = threadIdx.x; k < nu; k += NT) {
+                const int i = ul[k];
+                const T zi = q[i];
+                if (pcopy) pcopy[i] = zi;
+                rz += static_cast<double>(r[i]) * static_cast<double>(zi);
+                rr += static_cast<double>(r[i]) * static_cast<double>(r[i]);
+            }
             return;
         }
         // pre-smoothing from zero and the residual in one pass: z = w D^-1 r, q = r - A z (invd holds w / diag)
@@ -846,8 +862,13 @@ struct Win {
         prolong_add(0, z, LV<T>(1, nlev - 1 == 1 ? LV_X : LV_T));
         __syncthreads();
         mark(PH_V_PROLONG0);
-        unknowns2([&](int i) { return TPair{z[i] + invd[i] * (r[i] - apply0(gT, z, i)), T(0)}; },
-                  [&](int i, const TPair &v) { q[i] = v.a; });
+        unknowns2([&](int i) { return TPair{z[i] + invd[i] * (r[i] - apply0(gT, z, i)), r[i]}; },
+                  [&](int i, const TPair &v) {
+                      q[i] = v.a;
+                      if (pcopy) pcopy[i] = v.a;
+                      rz += static_cast<double>(v.b) * static_cast<double>(v.a);
+                      rr += static_cast<double>(v.b) * static_cast<double>(v.b);
+                  });
         __syncthreads();
         mark(PH_V_POST0);
     }
@@ -1037,15 +1058,8 @@ struct Win {
         double rz = 0.0, rr = 0.0;
         mark(PH_RESID);
         if (MG && use_mg) {
-            vcycle(r);
+            vcycle(r, rz, rr, p);
             mark(PH_VCYCLE);
-            for (int k = threadIdx.x; k < nu; k += NT) {
-                const int i = ul[k];
-                const T zi = q[i];
-                p[i] = zi;
-                rz += static_cast<double>(r[i]) * static_cast<double>(zi);
-                rr += static_cast<double>(r[i]) * static_cast<double>(r[i]);
-            }
         } else {
             for (int k = threadIdx.x; k < nu; k += NT) {
                 const int i = ul[k];
@@ -1082,13 +1096,8 @@ struct Win {
                 }
                 __syncthreads();  // the pre-smoothing reads r at the neighbours
                 mark(PH_CG);
-                vcycle(r);
+                vcycle(r, rz2, rr2);
                 mark(PH_VCYCLE);
-                for (int k = threadIdx.x; k < nu; k += NT) {
-                    const int i = ul[k];
-                    rz2 += static_cast<double>(r[i]) * static_cast<double>(q[i]);
-                    rr2 += static_cast<double>(r[i]) * static_cast<double>(r[i]);
-                }
             } else {
                 for (int k = threadIdx.x; k < nu; k += NT) {
                     const int i = ul[k];
@@ -1439,8 +1448,26 @@ struct Win {
     // slice origin.
     __device__ __forceinline__ void currents(double *out, const double *corr, int cy0, int cx0) {
         mark(PH_RESID);
-        const uint8_t *mask = A<uint8_t>(AR_MASK);
         const double *g64 = A<double>(AR_G64), *v = A<double>(AR_X64);
+        if (HOT && a.lay.stage != kNoStage) {
+            // the FP64 conductance and potentials live in global scratch; the solver's vectors and levels are
+            // dead now, so both are copied into that shared memory first (then every stencil read is on chip)
+            double *gs = reinterpret_cast<double *>(sm + a.lay.stage), *vs = gs + G.NP;
+            for (int i = threadIdx.x; i < G.NP; i += NT) {
+                gs[i] = g64[i];
+                vs[i] = v[i];
+            }
+            __syncthreads();
+            currents_from(gs, vs, out, corr, cy0, cx0);
+        } else {
+            currents_from(g64, v, out, corr, cy0, cx0);
+        }
+        mark(PH_CURRENTS);
+    }
+
+    __device__ __forceinline__ void currents_from(const double *g64, const double *v, double *out, const double *corr,
+                                                  int cy0, int cx0) {
+        const uint8_t *mask = A<uint8_t>(AR_MASK);
         const bool series = a.series;
         double maxout = -CUDART_INF, maxin = -CUDART_INF;
         for (int i = threadIdx.x; i < G.NP; i += NT) {
@@ -1481,7 +1508,6 @@ struct Win {
             out[y * G.w + x] = c;
         }
         __syncthreads();
-        mark(PH_CURRENTS);
     }
 };
 
