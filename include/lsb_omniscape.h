@@ -180,6 +180,42 @@ int64_t lsb_last_launch_count(void);
  * return stats: their device time goes to stats->window_ms (profiling aid; 0 = off, the default). */
 void lsb_time_window_kernels(int32_t on);
 
+/* ---------------------------------------------------------------------------
+ * Advanced mode on a batch of rasters: replaces circuit_advanced (src/cpp/circuit/python.cpp:65-80; engine
+ * circuit::advanced, src/cpp/circuit/grid.cpp:73-210) and solves many independent rasters in one launch.
+ * Every cell with conductance > 0 is a node joined to its 8 (or 4) neighbours by the average conductance; a
+ * source injects current; a ground connects its cell to 0 V through the given conductance (INFINITY: a direct
+ * ground, the cell held at 0 V); a grounded cell loses its source.  Each connected component with a nonzero
+ * source sum and a ground is solved; its node currents are max(inflow, outflow) with branch currents below 1e-8
+ * of the component's largest left out, and currents to finite grounds counted.  Voltage: the solution on solved
+ * components, 0 on the other nodes, NaN off the nodes; current 0 where nothing is solved.
+ *
+ * The n rasters are packed back to back in the device arrays conductance, source, ground (no NaN: the Python
+ * layer maps NaN to 0), current and voltage: raster k (ny[k] x nx[k], row-major) starts at the sum of the
+ * earlier rasters' cells.  nx and ny are host arrays; sides from 1 to 1024.
+ * ------------------------------------------------------------------------- */
+typedef struct lsb_raster_params {
+    int32_t four_neighbors; /* 0/1 */
+    int32_t precision;      /* lsb_precision: FP32 CG + FP64 refinement (multigrid) or FP64 CG (Jacobi) */
+    double tol;             /* relative FP64 residual at which a component is solved */
+    int32_t max_iter;       /* cap on CG iterations per component */
+    int32_t pad_;
+    double memory_limit;    /* bytes of solver scratch in global memory (0: 8 GiB); fewer CTAs when exceeded */
+} lsb_raster_params;
+
+/* Defaults: 8 neighbours, FP32 + refinement, tol 1e-12, max_iter 20000. */
+void lsb_raster_params_default(lsb_raster_params *p);
+
+/* Device bytes lsb_rasters needs for these raster sizes. */
+int lsb_rasters_workspace_size(int64_t n, const int32_t *nx, const int32_t *ny, const lsb_raster_params *p,
+                               size_t *bytes);
+
+/* Solves the batch on `stream`.  With stats != NULL the call waits for the stream and reports solver failures
+ * (LSB_ERR_NOT_CONVERGED); stats->n_targets is the number of rasters, n_solved those with a solved component. */
+int lsb_rasters(int64_t n, const int32_t *nx, const int32_t *ny, const double *conductance, const double *source,
+                const double *ground, const lsb_raster_params *p, double *current, double *voltage, void *workspace,
+                size_t workspace_bytes, lsb_omni_stats *stats, char *err, size_t errlen, void *stream);
+
 /* Tuning table (no counterpart in the reference): the preconditioner and threads per window that calls with
  * preconditioner = LSB_PC_AUTO or threads_per_window = 0 use for windows window_width = 2 (radius + buffer) + 1
  * cells wide, with these neighbours, edge weights and precision.  Entries come from an autotuning run

@@ -14,7 +14,8 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB = PKG / "liblsb_omni.so"
-SOURCES = [CSRC / "omni_capi.cu"] + [CSRC / f"omni_win_{nt}_{kind}.cu" for nt in (256, 512) for kind in ("hot", "gen")]
+SOURCES = ([CSRC / "omni_capi.cu", CSRC / "omni_adv.cu"] +
+           [CSRC / f"omni_win_{nt}_{kind}.cu" for nt in (256, 512) for kind in ("hot", "gen")])
 DEPS = SOURCES + sorted(CSRC.glob("*.cuh")) + [PKG.parent / "include" / "lsb_omniscape.h"]
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]

@@ -21,7 +21,7 @@ EDGE_AVERAGE, EDGE_SERIES = 0, 1
 EXPORTS = ("lsb_params_default", "lsb_omniscape_workspace_size", "lsb_omniscape", "lsb_omniscape_correction",
            "lsb_omniscape_grad", "lsb_omniscape_grad_workspace_size", "lsb_last_launch_count",
            "lsb_time_window_kernels", "lsb_version", "lsb_omniscape_noalloc", "lsb_tune_set", "lsb_tune_get",
-           "lsb_tune_clear")
+           "lsb_tune_clear", "lsb_raster_params_default", "lsb_rasters_workspace_size", "lsb_rasters")
 
 
 class Condition(C.Structure):
@@ -48,6 +48,11 @@ class Stats(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad_"}
+
+
+class RasterParams(C.Structure):
+    _fields_ = [("four_neighbors", C.c_int32), ("precision", C.c_int32), ("tol", C.c_double),
+                ("max_iter", C.c_int32), ("pad_", C.c_int32), ("memory_limit", C.c_double)]
 
 
 class NativeError(RuntimeError):
@@ -102,6 +107,13 @@ def load():
         lib.lsb_tune_get.restype = C.c_int
         lib.lsb_tune_clear.argtypes = []
         lib.lsb_tune_clear.restype = None
+        lib.lsb_raster_params_default.argtypes = [C.POINTER(RasterParams)]
+        lib.lsb_raster_params_default.restype = None
+        lib.lsb_rasters_workspace_size.argtypes = [i64, vp, vp, C.POINTER(RasterParams), C.POINTER(sz)]
+        lib.lsb_rasters_workspace_size.restype = C.c_int
+        lib.lsb_rasters.argtypes = [i64, vp, vp, vp, vp, vp, C.POINTER(RasterParams), vp, vp, vp, sz,
+                                    C.POINTER(Stats), C.c_char_p, sz, vp]
+        lib.lsb_rasters.restype = C.c_int
         _lib = lib
         return lib
 
@@ -109,6 +121,12 @@ def load():
 def default_params() -> Params:
     p = Params()
     load().lsb_params_default(C.byref(p))
+    return p
+
+
+def default_raster_params() -> RasterParams:
+    p = RasterParams()
+    load().lsb_raster_params_default(C.byref(p))
     return p
 
 

@@ -19,6 +19,7 @@
 
 #include "../../include/lsb_omniscape.h"
 #include "omni_kernels.cuh"
+#include "omni_adv.cuh"
 #include "omni_windows.cuh"
 
 namespace lsb {
@@ -181,17 +182,19 @@ constexpr size_t kStaticSmem = 3072;  // the window kernel's static shared memor
 constexpr size_t kStaticSmem = 2048;  // the window kernel's static shared memory, with room to spare
 #endif
 
-ArenaLayout make_layout(const Variant &v, int W, size_t smem_budget, bool grad) {
+// H x Wd: the largest box the launch solves (a window, or the largest raster of a batch: every level of a
+// smaller box fits the arrays of the larger); raster: the finite-ground arrays of the advanced mode.
+ArenaLayout make_layout(const Variant &v, int H, int Wd, size_t smem_budget, bool grad, bool raster = false) {
     ArenaLayout L;
     std::memset(&L, 0, sizeof L);
-    const size_t np = static_cast<size_t>(W + 2) * (W + 2);
+    const size_t np = static_cast<size_t>(H + 2) * (Wd + 2);
     const size_t ts = v.dbl ? 8 : 4;
     struct Item {
         int arr;
         size_t bytes;
     };
     std::vector<Item> items;  // in smem priority order
-    items.push_back({AR_ULIST, np * 2});
+    items.push_back({AR_ULIST, np * 4});
     items.push_back({AR_GT, np * ts});
     items.push_back({AR_P, np * ts});
     if (v.mg) items.push_back({AR_Z, np * ts});
@@ -201,8 +204,8 @@ ArenaLayout make_layout(const Variant &v, int W, size_t smem_budget, bool grad) 
     const bool has_d = !(v.dbl && !v.refine);
     if (has_d) items.push_back({AR_D, np * ts});
     if (v.mg) {
-        const int nlev = mg_levels(W, W);
-        int h = W, w = W;
+        const int nlev = mg_levels(H, Wd);
+        int h = H, w = Wd;
         for (int l = 1; l < nlev; ++l) {
             h = coarse_dim(h);
             w = coarse_dim(w);
@@ -211,11 +214,13 @@ ArenaLayout make_layout(const Variant &v, int W, size_t smem_budget, bool grad) 
         }
         items.push_back({AR_DENSE, static_cast<size_t>(kNcMax) * (kNcMax + 2) * 8});  // + pivot column, diagonal
     }
+    if (raster) items.push_back({AR_FGT, np * ts});
     items.push_back({AR_MASK, np});
     if (!has_d) items.push_back({AR_X64, np * 8});  // the solution is the iterate: keep it close
     if (has_d) items.push_back({AR_X64, np * 8});
     items.push_back({AR_G64, np * 8});
     items.push_back({AR_B64, np * 8});
+    if (raster) items.push_back({AR_FG64, np * 8});
     if (grad) {
         items.push_back({AR_V64, np * 8});
         items.push_back({AR_CW, np * 8});
@@ -307,7 +312,7 @@ int make_plan(int64_t nx, int64_t ny, const lsb_omni_params *p, Plan *pl, char *
     DeviceInfo di;
     LSB_CK(device_info(&di));
     const size_t budget = di.smem_optin > kStaticSmem ? di.smem_optin - kStaticSmem : 0;
-    pl->lay = make_layout(pl->v, g.W, budget, grad);
+    pl->lay = make_layout(pl->v, g.W, g.W, budget, grad);
     pl->kern = pick(pl->v, pl->lay.hot != 0);
     LSB_CK(cudaFuncSetAttribute(reinterpret_cast<const void *>(pl->kern),
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(pl->lay.smem_bytes)));
@@ -509,6 +514,95 @@ int enqueue(const Plan &pl, const double *res, const double *src, const lsb_omni
 }  // namespace lsb
 
 using namespace lsb;
+
+// ---------------------------------------------------------------------------
+// Raster batches (advanced mode).
+// ---------------------------------------------------------------------------
+constexpr int kMaxRasterSide = 1024;  // nine multigrid levels; padded indices below 2^22
+
+struct RasterPlan {
+    Variant v;
+    ArenaLayout lay;
+    KernelFn kern;
+    int grid;
+    int64_t n, cells;
+    std::vector<int64_t> off;
+    std::vector<int> order;
+    size_t o_off, o_nx, o_ny, o_order, o_queue, o_count, o_stat, o_devstats, o_gs, total;
+};
+
+int raster_plan(int64_t n, const int32_t *nx, const int32_t *ny, const lsb_raster_params *p, RasterPlan *pl,
+                char *err, size_t errlen) {
+    if (!p || !nx || !ny || n < 1 || n > (1 << 30)) {
+        set_err(err, errlen, "expected at least one raster, its sizes and parameters");
+        return LSB_ERR_ARGUMENT;
+    }
+    if (p->precision != LSB_PREC_FP64 && p->precision != LSB_PREC_FP32_REFINE) {
+        set_err(err, errlen, "precision must be LSB_PREC_FP64 or LSB_PREC_FP32_REFINE");
+        return LSB_ERR_ARGUMENT;
+    }
+    int H = 1, Wd = 1;
+    pl->n = n;
+    pl->off.resize(static_cast<size_t>(n));
+    pl->cells = 0;
+    for (int64_t k = 0; k < n; ++k) {
+        if (nx[k] < 1 || ny[k] < 1 || nx[k] > kMaxRasterSide || ny[k] > kMaxRasterSide) {
+            set_err(err, errlen, "raster %lld is %d x %d: sides must be 1..%d", static_cast<long long>(k), ny[k],
+                    nx[k], kMaxRasterSide);
+            return LSB_ERR_ARGUMENT;
+        }
+        pl->off[k] = pl->cells;
+        pl->cells += static_cast<int64_t>(nx[k]) * ny[k];
+        H = std::max<int>(H, ny[k]);
+        Wd = std::max<int>(Wd, nx[k]);
+    }
+    // the largest rasters first, so that the persistent CTAs finish together
+    pl->order.resize(static_cast<size_t>(n));
+    for (int64_t k = 0; k < n; ++k) pl->order[k] = static_cast<int>(k);
+    std::stable_sort(pl->order.begin(), pl->order.end(), [&](int a, int b) {
+        return static_cast<int64_t>(nx[a]) * ny[a] > static_cast<int64_t>(nx[b]) * ny[b];
+    });
+    Variant &v = pl->v;
+    v.four = p->four_neighbors != 0;
+    v.dbl = p->precision == LSB_PREC_FP64;
+    v.refine = !v.dbl;
+    v.mg = !v.dbl;
+    v.pc = v.dbl ? LSB_PC_JACOBI : LSB_PC_MG;
+    v.nt = 512;
+    DeviceInfo di;
+    LSB_CK(device_info(&di));
+    const size_t budget = di.smem_optin > kStaticSmem ? di.smem_optin - kStaticSmem : 0;
+    pl->lay = make_layout(v, H, Wd, budget, false, true);
+    pl->kern = pick_rasters(pl->lay.hot != 0, v.four, v.dbl);
+    LSB_CK(cudaFuncSetAttribute(reinterpret_cast<const void *>(pl->kern),
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(pl->lay.smem_bytes)));
+    int per_sm = 0;
+    LSB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pl->kern, v.nt, pl->lay.smem_bytes));
+    if (per_sm < 1) {
+        set_err(err, errlen, "the raster kernel does not fit on an SM (%u bytes of shared memory)", pl->lay.smem_bytes);
+        return LSB_ERR_ARGUMENT;
+    }
+    const double lim = p->memory_limit > 0 ? p->memory_limit : 8.0 * (1 << 30);
+    const int64_t by_mem = std::max<int64_t>(1, static_cast<int64_t>(lim / std::max<double>(pl->lay.gmem_bytes, 1)));
+    pl->grid = static_cast<int>(std::min<int64_t>(std::min<int64_t>(static_cast<int64_t>(di.sms) * per_sm, n), by_mem));
+    size_t o = 0;
+    auto take = [&](size_t bytes) {
+        const size_t r = o;
+        o += align_up(std::max<size_t>(bytes, 1));
+        return r;
+    };
+    pl->o_off = take(n * 8);
+    pl->o_nx = take(n * 4);
+    pl->o_ny = take(n * 4);
+    pl->o_order = take(n * 4);
+    pl->o_queue = take(4);
+    pl->o_count = take(4);
+    pl->o_stat = take(n * sizeof(WinStat));
+    pl->o_devstats = take(sizeof(DevStats));
+    pl->o_gs = take(static_cast<size_t>(pl->grid) * pl->lay.gmem_bytes);
+    pl->total = o;
+    return LSB_OK;
+}
 
 extern "C" {
 
@@ -966,6 +1060,101 @@ int lsb_omniscape_grad(const double *resistance, const double *source, const dou
 int64_t lsb_last_launch_count(void) { return g_launches; }
 
 void lsb_time_window_kernels(int32_t on) { g_time_windows = on != 0; }
+
+void lsb_raster_params_default(lsb_raster_params *p) {
+    std::memset(p, 0, sizeof *p);
+    p->precision = LSB_PREC_FP32_REFINE;
+    p->tol = 1e-12;
+    p->max_iter = 20000;
+}
+
+int lsb_rasters_workspace_size(int64_t n, const int32_t *nx, const int32_t *ny, const lsb_raster_params *p,
+                               size_t *bytes) {
+    RasterPlan pl;
+    const int rc = raster_plan(n, nx, ny, p, &pl, nullptr, 0);
+    if (rc) return rc;
+    *bytes = pl.total;
+    return LSB_OK;
+}
+
+int lsb_rasters(int64_t n, const int32_t *nx, const int32_t *ny, const double *conductance, const double *source,
+                const double *ground, const lsb_raster_params *p, double *current, double *voltage, void *workspace,
+                size_t workspace_bytes, lsb_omni_stats *stats, char *err, size_t errlen, void *stream) {
+    RasterPlan pl;
+    int rc = raster_plan(n, nx, ny, p, &pl, err, errlen);
+    if (rc) return rc;
+    if (!conductance || !source || !ground || !current || !voltage) {
+        set_err(err, errlen, "conductance, source, ground, current and voltage are required");
+        return LSB_ERR_ARGUMENT;
+    }
+    if (!workspace || workspace_bytes < pl.total) {
+        set_err(err, errlen, "workspace too small: %zu bytes needed", pl.total);
+        return LSB_ERR_WORKSPACE;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    char *ws = static_cast<char *>(workspace);
+    const int count = static_cast<int>(n);
+    // descriptors (pageable host memory: each copy is staged before the call returns)
+    LSB_CK(cudaMemcpyAsync(ws + pl.o_off, pl.off.data(), n * 8, cudaMemcpyHostToDevice, s));
+    LSB_CK(cudaMemcpyAsync(ws + pl.o_nx, nx, n * 4, cudaMemcpyHostToDevice, s));
+    LSB_CK(cudaMemcpyAsync(ws + pl.o_ny, ny, n * 4, cudaMemcpyHostToDevice, s));
+    LSB_CK(cudaMemcpyAsync(ws + pl.o_order, pl.order.data(), n * 4, cudaMemcpyHostToDevice, s));
+    LSB_CK(cudaMemcpyAsync(ws + pl.o_count, &count, 4, cudaMemcpyHostToDevice, s));
+    LSB_CK(cudaMemsetAsync(ws + pl.o_queue, 0, 4, s));
+    KArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.res = conductance;
+    a.src = source;
+    a.gnd = ground;
+    a.four = pl.v.four;
+    a.cur_win = current;
+    a.fp_win = voltage;
+    a.stat = reinterpret_cast<WinStat *>(ws + pl.o_stat);
+    a.queue = reinterpret_cast<int *>(ws + pl.o_queue);
+    a.gscratch = ws + pl.o_gs;
+    a.lay = pl.lay;
+    lsb_omni_params q;
+    lsb_params_default(&q);
+    q.precision = p->precision;
+    q.tol = p->tol;
+    q.max_iter = p->max_iter;
+    a.sp = solve_params(&q, pl.v.pc);
+    a.mode = 3;
+    a.ras_off = reinterpret_cast<const int64_t *>(ws + pl.o_off);
+    a.ras_nx = reinterpret_cast<const int *>(ws + pl.o_nx);
+    a.ras_ny = reinterpret_cast<const int *>(ws + pl.o_ny);
+    a.ras_order = reinterpret_cast<const int *>(ws + pl.o_order);
+    a.n_rasters = count;
+    pl.kern<<<pl.grid, pl.v.nt, pl.lay.smem_bytes, s>>>(a);
+    LSB_CK(cudaGetLastError());
+    k_stats<<<1, 1024, 0, s>>>(a.stat, reinterpret_cast<const int *>(ws + pl.o_count), 1,
+                               reinterpret_cast<DevStats *>(ws + pl.o_devstats));
+    LSB_CK(cudaGetLastError());
+    g_launches = 2;
+    if (stats) {
+        DevStats ds;
+        LSB_CK(cudaMemcpyAsync(&ds, ws + pl.o_devstats, sizeof ds, cudaMemcpyDeviceToHost, s));
+        LSB_CK(cudaStreamSynchronize(s));
+        std::memset(stats, 0, sizeof *stats);
+        stats->n_targets = n;
+        stats->n_solved = ds.n_solved;
+        stats->n_failed = ds.n_failed;
+        stats->iters_total = ds.iters_total;
+        stats->iters_max = ds.iters_max;
+        stats->refine_max = ds.refine_max;
+        stats->batches = 1;
+        stats->threads_per_window = pl.v.nt;
+        stats->preconditioner = pl.v.pc;
+        stats->worst_residual = ds.worst_residual;
+        stats->unknown_iters = ds.unknown_iters;
+        if (ds.n_failed > 0) {
+            set_err(err, errlen, "%lld raster solves did not converge (worst relative residual %.3g)",
+                    static_cast<long long>(ds.n_failed), ds.worst_residual);
+            return LSB_ERR_NOT_CONVERGED;
+        }
+    }
+    return LSB_OK;
+}
 
 int lsb_tune_set(int32_t window_width, int32_t four_neighbors, int32_t edge_weights, int32_t precision,
                  int32_t preconditioner, int32_t threads_per_window) {

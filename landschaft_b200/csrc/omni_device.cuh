@@ -92,7 +92,8 @@ struct WinGeom {
 };
 
 // Mask bits of a level-0 cell.
-enum : uint8_t { M_UNKNOWN = 1, M_PRESENT = 2, M_CAND = 4, M_USEIN = 8 };
+enum : uint8_t { M_UNKNOWN = 1, M_PRESENT = 2, M_CAND = 4, M_USEIN = 8, M_DIRECT = 16, M_DONE = 32 };
+// (M_DIRECT: a direct ground of a raster solve; M_DONE: the cell's component has been handled)
 
 constexpr int kMaxLevels = 9;  // level 0 + up to 8 coarse levels (windows up to 513 cells wide)
 constexpr int kNcMax = 25;     // cells of the coarsest level (solved by its dense inverse)
@@ -101,7 +102,7 @@ constexpr int kNcMax = 25;     // cells of the coarsest level (solved by its den
 enum LevelArray : int { LV_C0 = 0, LV_CE, LV_CSW, LV_CS, LV_CSE, LV_INVD, LV_X, LV_B, LV_T, LV_COUNT };
 enum ArenaArray : int {
     AR_MASK = 0,  // u8
-    AR_ULIST,     // u16: padded indices of the unknowns, row-major
+    AR_ULIST,     // u32: padded indices of the unknowns, row-major
     AR_G64,       // f64: conductance (-9999 outside / NoData; 0 on padding)
     AR_X64,       // f64: solution (potentials), 0 off the unknowns
     AR_B64,       // f64: scaled sources (the right-hand side)
@@ -116,6 +117,8 @@ enum ArenaArray : int {
     AR_Q,         // T: A p; multigrid fine residual and output
     AR_Z,         // T: multigrid pre-smoothed residual; the fine diagonal during set-up
     AR_DENSE,     // f64: inverse of the coarsest operator (kNcMax^2)
+    AR_FG64,      // f64: finite ground conductance of a raster solve (0 elsewhere)
+    AR_FGT,       // T: the same for the inner operator
     AR_LEVEL,     // first coarse level; each coarse level has LV_COUNT arrays
     AR_COUNT = AR_LEVEL + (kMaxLevels - 1) * LV_COUNT
 };

@@ -28,8 +28,8 @@ struct KArgs {
     const double *lat_amps; // per lattice point: the block's source sum
     const double *corr;     // W x W correction factors, or null
     // outputs of a batch
-    double *cur_win;  // batch slots of W*W doubles (pitch w of each window)
-    double *fp_win;
+    double *cur_win;  // batch slots of W*W doubles (pitch w of each window); raster solves: the current maps
+    double *fp_win;   // raster solves: the voltage maps
     WinStat *stat;    // per target: [land, flow]
     int *queue;       // work counter of this launch
     int batch_start, batch_size;
@@ -44,7 +44,15 @@ struct KArgs {
     // per-phase cycle counters (builds with LSB_PHASE_TIMERS only)
     unsigned long long *timers;
     double *Jw;  // mode 2: J's share of every target
+    // raster solves (advanced mode): ground rasters, and per raster its offset in the packed maps, its width and
+    // height; the queue visits rasters in `order`
+    const double *gnd;
+    const int64_t *ras_off;
+    const int *ras_nx, *ras_ny, *ras_order;
+    int n_rasters;
 };
+
+using KernelFn = void (*)(const KArgs);
 
 // Phases of a window solve, for the cycle counters of profiling builds.
 enum Phase : int { PH_LOAD = 0, PH_FLOOD, PH_MARK, PH_ASSEMBLE, PH_MG_SETUP, PH_RESID, PH_CG, PH_VCYCLE, PH_CURRENTS,
@@ -82,7 +90,7 @@ __device__ __forceinline__ double tmax(double a, double b) { return fmax(a, b); 
 // Block-wide ordered compaction of flags over [0, n): out[k] = i of the k-th
 // flagged i (increasing).  Returns the count.  scan: shared, >= 33 ints.
 template <int NT, typename F>
-__device__ __forceinline__ int block_compact(int n, F flag, uint16_t *out, int *scan) {
+__device__ __forceinline__ int block_compact(int n, F flag, uint32_t *out, int *scan) {
     constexpr int NW = NT / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int base = 0;
@@ -99,7 +107,7 @@ __device__ __forceinline__ int block_compact(int n, F flag, uint16_t *out, int *
             before += k < warp ? c : 0;
             total += c;
         }
-        if (f) out[base + before + __popc(m & ((1u << lane) - 1u))] = static_cast<uint16_t>(i);
+        if (f) out[base + before + __popc(m & ((1u << lane) - 1u))] = static_cast<uint32_t>(i);
         base += total;
         __syncthreads();
     }
@@ -111,12 +119,14 @@ __device__ __forceinline__ int block_compact(int n, F flag, uint16_t *out, int *
 // ---------------------------------------------------------------------------
 // Arrays a window keeps in shared memory whenever the layout's HOT flag is set: all but the FP64 window arrays.
 __host__ __device__ constexpr bool hot_array(int k) {
-    return !(k == AR_X64 || k == AR_G64 || k == AR_B64 || k == AR_V64 || k == AR_CW || k == AR_DG64);
+    return !(k == AR_X64 || k == AR_G64 || k == AR_B64 || k == AR_V64 || k == AR_CW || k == AR_DG64 || k == AR_FG64);
 }
 
 // HOT: every hot array of the layout is in shared memory, so their pointers derive from the shared-memory base and
 // compile to 32-bit shared addressing (else each pointer is chosen at run time and addressed generically).
-template <int NT, typename T, bool FOUR, bool MG, bool REFINE, bool HOT>
+// ADV: a whole-raster solve of the advanced mode (grid.cpp:73-210) instead of a moving window: finite grounds add
+// their conductance to the diagonal, direct grounds are not unknowns, and the components are solved one by one.
+template <int NT, typename T, bool FOUR, bool MG, bool REFINE, bool HOT, bool ADV = false>
 struct Win {
     static_assert(REFINE || sizeof(T) == 8, "an FP32 inner solve needs the FP64 refinement");
     using NB = Nb<FOUR>;
@@ -289,7 +299,7 @@ struct Win {
         // words); it is monotone, so words written during a sweep may be read old or new, and the sweeps end
         // when one changes nothing: pb is then the ground's component.
         const int P = G.P, words = (P + 31) >> 5, nrow = G.h + 2, ntask = nrow * words;
-        const float invwd = 1.0f / static_cast<float>(words);  // (k + 0.5) / words in float: exact row, k < 2^16
+        const float invwd = 1.0f / static_cast<float>(words);  // (k + 0.5) / words in float: exact row, k < 2^22
         uint32_t *cb = reinterpret_cast<uint32_t *>(A<T>(AR_P)), *pb = cb + ntask;
         const int gpy = G.gy + 1, gpx = G.gx + 1;
         const int lane = threadIdx.x & 31;
@@ -348,14 +358,14 @@ struct Win {
         double t = 0.0;
         for (int i = threadIdx.x; i < G.NP; i += NT) {
             uint8_t m = mask[i];
-            if ((m & M_PRESENT) && i != ground) {
+            if ((m & M_PRESENT) && (ADV ? !(m & M_DIRECT) : i != ground)) {
                 m |= M_UNKNOWN;
                 t += b64[i];
             }
             mask[i] = m;
         }
         const double total = red.sum(t);
-        nu = block_compact<NT>(G.NP, [&](int i) { return (mask[i] & M_UNKNOWN) != 0; }, A<uint16_t>(AR_ULIST), scan);
+        nu = block_compact<NT>(G.NP, [&](int i) { return (mask[i] & M_UNKNOWN) != 0; }, A<uint32_t>(AR_ULIST), scan);
         return total;
     }
 
@@ -379,9 +389,10 @@ struct Win {
             r[i] = T(0);
             if (!(REFINE == false && sizeof(T) == 8)) d[i] = T(0);
             if (MG) z[i] = T(0);
+            if (ADV) A<T>(AR_FGT)[i] = static_cast<T>(A<double>(AR_FG64)[i]);
         }
         __syncthreads();
-        const uint16_t *ul = A<uint16_t>(AR_ULIST);
+        const uint32_t *ul = A<uint32_t>(AR_ULIST);
         for (int k = threadIdx.x; k < nu; k += NT) {
             const int i = ul[k];
             const double gi = g64[i];
@@ -391,6 +402,7 @@ struct Win {
                 const int n = i + noff(dd);
                 if (mask[n] & M_PRESENT) diag += edge_w64(gi, g64[n], NB::diag(dd), series);
             }
+            if (ADV) diag += A<double>(AR_FG64)[i];  // a finite ground (system.cpp: the extra diagonal)
             // multigrid kernels keep omega / diag: the damped-Jacobi smoother's factor (a scalar multiple of
             // the Jacobi preconditioner, to which CG is invariant)
             invd[i] = static_cast<T>((MG ? static_cast<double>(a.sp.omega) : 1.0) / (diag + kShift));
@@ -412,7 +424,7 @@ struct Win {
     // the two cells' memory latencies overlap.
     template <class C, class Put>
     __device__ __forceinline__ void unknowns2(C calc, Put put) const {
-        const uint16_t *ul = A<uint16_t>(AR_ULIST);
+        const uint32_t *ul = A<uint32_t>(AR_ULIST);
         for (int k = threadIdx.x; k < nu; k += 2 * NT) {
             const bool two = k + NT < nu;
             const int i1 = ul[k], i2 = two ? ul[k + NT] : i1;
@@ -439,7 +451,7 @@ struct Win {
                 else
                     ao += wv * (xi - x[n]);
             }
-            return ao + ad * T(0.70710678118654752440);
+            return ao + ad * T(0.70710678118654752440) + (ADV ? A<T>(AR_FGT)[i] * xi : T(0));
         }
 #pragma unroll
         for (int dd = 0; dd < ND; ++dd) {
@@ -450,7 +462,7 @@ struct Win {
             else
                 ao += wv * (xi - x[n]);
         }
-        return ao * T(0.5) + ad * T(kInvTwoSqrt2);
+        return ao * T(0.5) + ad * T(kInvTwoSqrt2) + (ADV ? A<T>(AR_FGT)[i] * xi : T(0));
     }
 
     // A level-0 entry A(i, i+s) for RAP (s = (sy, sx) in {-1,0,1}^2).
@@ -561,7 +573,8 @@ struct Win {
     // diagonal and the 4 entries towards E, SW, S, SE (the rest by symmetry).
 
     // Cells of level l, warps along rows and lanes along columns (no division).
-    // (k + 0.5) / w in float gives the exact row of cell k (k < h w <= 65536, quotient < 257).
+    // (k + 0.5) / w in float gives the exact row of cell k whenever k + 0.5 < 2^22: the rounding error, at most
+    // 2^-23 of the quotient, stays below the quotient's distance 0.5 / w from an integer.
     template <class F>
     __device__ __forceinline__ void for_cells(int l, F f) const {
         const int h = lvh[l], w = lvw[l], P = w + 2, n = h * w;
@@ -805,7 +818,7 @@ struct Win {
         __syncthreads();
     }
 
-    // Row of a padded index of level 0 (i < 65536, 3 <= P <= 256): exact in float.
+    // Row of a padded index of level 0 (i < 2^22, as for_cells): exact in float.
     __device__ __forceinline__ int row0(int i) const {
         return static_cast<int>((static_cast<float>(i) + 0.5f) * invP);
     }
@@ -815,7 +828,7 @@ struct Win {
     // Also adds this thread's terms of r.z and r.r to rz and rr (its unknowns in increasing order), and copies z
     // to pcopy when given.
     __device__ __forceinline__ void vcycle(const T *r, double &rz, double &rr, T *pcopy = nullptr) {
-        const uint16_t *ul = A<uint16_t>(AR_ULIST);
+        const uint32_t *ul = A<uint32_t>(AR_ULIST);
         const T *gT = A<T>(AR_GT), *invd = A<T>(AR_INVD);
         T *z = A<T>(AR_Z), *q = A<T>(AR_Q);
         if (nlev == 1) {
@@ -889,7 +902,7 @@ struct Win {
                 else
                     ao += wv * (zi - zn);
             }
-            return ao + ad * T(0.70710678118654752440);
+            return ao + ad * T(0.70710678118654752440) + (ADV ? A<T>(AR_FGT)[i] * zi : T(0));
         }
 #pragma unroll
         for (int dd = 0; dd < ND; ++dd) {
@@ -901,7 +914,7 @@ struct Win {
             else
                 ao += wv * (zi - zn);
         }
-        return ao * T(0.5) + ad * T(kInvTwoSqrt2);
+        return ao * T(0.5) + ad * T(kInvTwoSqrt2) + (ADV ? A<T>(AR_FGT)[i] * zi : T(0));
     }
 
     // b_{l} = P^T t_{l-1} (level l-1 residual, zero off its active cells); ends with a barrier.
@@ -1051,7 +1064,7 @@ struct Win {
     // most maxit iterations.
     // Returns the iterations; *ok = false on breakdown.
     __device__ __forceinline__ int pcg(T *d, T *r, double rtol, int maxit, bool use_mg, bool *ok) {
-        const uint16_t *ul = A<uint16_t>(AR_ULIST);
+        const uint32_t *ul = A<uint32_t>(AR_ULIST);
         const T *gT = A<T>(AR_GT), *invd = A<T>(AR_INVD);
         T *p = A<T>(AR_P), *q = A<T>(AR_Q);
         *ok = true;
@@ -1137,7 +1150,7 @@ struct Win {
     // reciprocal of 2 sqrt 2), stored as T in AR_R; returns (||r||^2, ||b||^2).
     __device__ __forceinline__ void residual64(double *rr_out, double *bb_out, bool first) {
         const uint8_t *mask = A<uint8_t>(AR_MASK);
-        const uint16_t *ul = A<uint16_t>(AR_ULIST);
+        const uint32_t *ul = A<uint32_t>(AR_ULIST);
         const double *g64 = A<double>(AR_G64), *x64 = A<double>(AR_X64), *b64 = A<double>(AR_B64);
         T *r = A<T>(AR_R);
         const bool series = a.series;
@@ -1164,7 +1177,7 @@ struct Win {
                             ao += wv * (xi - xn);
                     }
                     const double ax = series ? ao + ad * (1.0 / kSqrt2) : ao * 0.5 + ad * kInvTwoSqrt2;
-                    ri = bi - (ax + kShift * xi);
+                    ri = ADV ? bi - (ax + (A<double>(AR_FG64)[i] + kShift) * xi) : bi - (ax + kShift * xi);
                 }
                 return DPair{ri, bi};
             },
@@ -1182,7 +1195,7 @@ struct Win {
     // x64 must be zero on entry; with setup == false the multigrid hierarchy of the previous solve of the same
     // matrix is reused.
     __device__ __forceinline__ void solve(WinStat *st, bool setup = true) {
-        const uint16_t *ul = A<uint16_t>(AR_ULIST);
+        const uint32_t *ul = A<uint32_t>(AR_ULIST);
         double *x64 = A<double>(AR_X64);
         const bool want_mg = MG && a.sp.pc == 2;
         mark(PH_ASSEMBLE);
@@ -1502,11 +1515,161 @@ struct Win {
                         if (!(fabs(b / maxout) < 1e-8)) outflow -= b;
                     }
                 }
+                if (ADV) {
+                    // current to a finite ground, never thresholded (grid.cpp:19-71)
+                    const double f = A<double>(AR_FG64)[i] * vi;
+                    if (f < 0)
+                        inflow -= f;
+                    else if (f > 0)
+                        outflow += f;
+                }
                 c = inflow > outflow ? inflow : outflow;
                 if (corr) c *= corr[(cy0 + y) * W + (cx0 + x)];
+                if (ADV) volt_out[y * G.w + x] = vi;
             }
-            out[y * G.w + x] = c;
+            if (!ADV || (mask[i] & M_PRESENT)) out[y * G.w + x] = c;  // a raster solve writes its component only
         }
+        __syncthreads();
+    }
+
+    // ---- whole-raster solves (advanced mode, grid.cpp:73-210) -------------------------------------------------
+    double *volt_out = nullptr;  // the raster's voltage map (pitch w)
+
+    // Conductance (a node where > 0), sources (0 where the cell is also grounded), finite and direct grounds of
+    // the raster at g, s, gr (h x w, pitch w); the outputs start as current 0 and voltage 0 on nodes, NaN off
+    // them.  (The reference adds the finite grounds to the diagonal when any is nonzero; zero entries change
+    // nothing, so they are always added here.)
+    __device__ __forceinline__ void load_raster(const double *g, const double *s, const double *gr, double *cur) {
+        uint8_t *mask = A<uint8_t>(AR_MASK);
+        double *g64 = A<double>(AR_G64), *x64 = A<double>(AR_X64), *b64 = A<double>(AR_B64),
+               *fg = A<double>(AR_FG64);
+        const int P = G.P;
+        invP = 1.0f / static_cast<float>(P);
+        for (int i = threadIdx.x; i < G.NP; i += NT) {
+            const int py = row0(i), y = py - 1, x = i - py * P - 1;
+            double gi = 0.0, si = 0.0, fi = 0.0;
+            uint8_t m = 0;
+            if (y >= 0 && y < G.h && x >= 0 && x < G.w) {
+                const int c = y * G.w + x;
+                gi = g[c];
+                const bool node = gi > 0;
+                cur[c] = 0.0;
+                volt_out[c] = node ? 0.0 : CUDART_NAN;
+                if (node) {
+                    m = M_CAND;
+                    const double gc = gr[c];
+                    si = s[c];
+                    if (gc != 0) si = 0.0;  // a grounded cell loses its source
+                    if (gc == CUDART_INF)
+                        m |= M_DIRECT;
+                    else
+                        fi = gc;
+                } else {
+                    gi = -9999.0;  // no node (never read as a conductance)
+                }
+            }
+            mask[i] = m;
+            g64[i] = gi;
+            b64[i] = si;
+            fg[i] = fi;
+            x64[i] = 0.0;
+        }
+        __syncthreads();
+    }
+
+    // Smallest padded index of a node whose component is not handled yet, or -1.
+    __device__ __forceinline__ int next_seed() {
+        const uint8_t *mask = A<uint8_t>(AR_MASK);
+        int best = 0x7fffffff;
+        for (int i = threadIdx.x; i < G.NP; i += NT)
+            if ((mask[i] & (M_CAND | M_DONE)) == M_CAND) {
+                best = i;
+                break;
+            }
+        scan[0] = 0x7fffffff;
+        __syncthreads();
+        atomicMin(&scan[0], best);
+        __syncthreads();
+        const int s = scan[0];
+        __syncthreads();
+        return s == 0x7fffffff ? -1 : s;
+    }
+
+    // The component of `seed` among the nodes not handled yet: bit rows as in flood(); its cells get M_PRESENT
+    // and M_DONE.
+    __device__ __forceinline__ void flood_from(int seed) {
+        uint8_t *mask = A<uint8_t>(AR_MASK);
+        const int P = G.P, words = (P + 31) >> 5, nrow = G.h + 2, ntask = nrow * words;
+        const float invwd = 1.0f / static_cast<float>(words);
+        uint32_t *cb = reinterpret_cast<uint32_t *>(A<T>(AR_P)), *pb = cb + ntask;
+        const int spy = row0(seed), spx = seed - spy * P;
+        const int lane = threadIdx.x & 31;
+        for (int k = threadIdx.x >> 5; k < ntask; k += NT / 32) {
+            const int py = static_cast<int>((static_cast<float>(k) + 0.5f) * invwd), w = k - py * words;
+            const int px = 32 * w + lane;
+            const bool c = px < P && (mask[py * P + px] & (M_CAND | M_DONE)) == M_CAND;
+            const uint32_t bits = __ballot_sync(0xffffffffu, c);
+            if (lane == 0) {
+                cb[k] = bits;
+                pb[k] = (py == spy && w == (spx >> 5)) ? (1u << (spx & 31)) : 0u;
+            }
+        }
+        __syncthreads();
+        volatile uint32_t *vp = pb;
+        while (true) {
+            int changed = 0;
+            for (int k = threadIdx.x; k < ntask; k += NT) {
+                const uint32_t c = cb[k];
+                if (!c) continue;
+                const int py = static_cast<int>((static_cast<float>(k) + 0.5f) * invwd), w = k - py * words;
+                const uint32_t mid = vp[k];
+                const bool hl = w > 0, hr = w + 1 < words;
+                uint32_t nb;
+                if (FOUR) {
+                    const uint32_t l = hl ? vp[k - 1] : 0u, r = hr ? vp[k + 1] : 0u;
+                    nb = vp[k - words] | vp[k + words] | (mid << 1) | (l >> 31) | (mid >> 1) | (r << 31);
+                } else {
+                    const uint32_t v = vp[k - words] | mid | vp[k + words];
+                    const uint32_t vl = hl ? (vp[k - words - 1] | vp[k - 1] | vp[k + words - 1]) : 0u;
+                    const uint32_t vr = hr ? (vp[k - words + 1] | vp[k + 1] | vp[k + words + 1]) : 0u;
+                    nb = v | (v << 1) | (vl >> 31) | (v >> 1) | (vr << 31);
+                }
+                (void)py;
+                const uint32_t nw = c & (mid | nb);
+                if (nw != mid) {
+                    vp[k] = nw;
+                    changed = 1;
+                }
+            }
+            if (!__syncthreads_or(changed)) break;
+        }
+        for (int i = threadIdx.x; i < G.NP; i += NT) {
+            const int py = row0(i), px = i - py * P;
+            const uint8_t m = mask[i] & static_cast<uint8_t>(~(M_PRESENT | M_UNKNOWN));
+            mask[i] = ((pb[py * words + (px >> 5)] >> (px & 31)) & 1u) ? (m | M_PRESENT | M_DONE) : m;
+        }
+        __syncthreads();
+    }
+
+    // The component's source sum and whether it has a ground (a direct one, or finite ones summing to nonzero).
+    __device__ __forceinline__ bool component_active() {
+        const uint8_t *mask = A<uint8_t>(AR_MASK);
+        const double *b64 = A<double>(AR_B64), *fg = A<double>(AR_FG64);
+        double s = 0.0, gs = 0.0;
+        for (int i = threadIdx.x; i < G.NP; i += NT) {
+            const uint8_t m = mask[i];
+            if (!(m & M_PRESENT)) continue;
+            s += b64[i];
+            gs += (m & M_DIRECT) ? CUDART_INF : fg[i];
+        }
+        red.sum2(s, gs);
+        return s != 0 && gs != 0;
+    }
+
+    // After a component: its potentials back to zero (the next solve starts from x = 0).
+    __device__ __forceinline__ void clear_solution() {
+        double *x64 = A<double>(AR_X64);
+        for (int i = threadIdx.x; i < G.NP; i += NT) x64[i] = 0.0;
         __syncthreads();
     }
 };

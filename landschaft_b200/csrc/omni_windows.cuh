@@ -8,7 +8,6 @@
 
 namespace lsb {
 
-using KernelFn = void (*)(const KArgs);
 
 // ---------------------------------------------------------------------------
 // The persistent window solver.

@@ -12,6 +12,9 @@ All rasters are float64, row-major, NaN = NoData, drawn with ``numpy.random.defa
   cumulative current over rows and columns 224-287.
 * ``omni_4096`` -- 4096 x 4096 field with exponent -2.5, resistance 500^g in [1, 500], 5% NoData as random
   polygons, source 1 / resistance above the 40th percentile of resistance, else 0; radius 64, block 5.
+* ``advanced_rasters`` -- independent grounded raster circuits (the advanced mode): sides drawn uniformly from
+  64 to 512, resistance log-uniform in [1, 1000] (conductance 1 / resistance), one unit current source and one
+  direct ground at two distinct random cells; 4 neighbours.
 """
 
 from __future__ import annotations
@@ -112,6 +115,22 @@ def omni_4096(seed: int = 0):
     s = np.where(r > p40, 1.0 / r, 0.0)
     s[np.isnan(s)] = 0.0
     return r, s, dict(radius=64, block_size=5, buffer=0, four_neighbors=False)
+
+
+def advanced_rasters(n=4096, seed=0, side_min=64, side_max=512):
+    """(conductance, source, ground) triples of the advanced-mode batch."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        ny, nx = (int(v) for v in rng.integers(side_min, side_max + 1, 2))
+        r = np.exp(rng.uniform(np.log(1.0), np.log(1000.0), (ny, nx)))
+        s = np.zeros((ny, nx))
+        gr = np.zeros((ny, nx))
+        a, b = rng.choice(ny * nx, 2, replace=False)
+        s.flat[a] = 1.0
+        gr.flat[b] = np.inf
+        out.append((1.0 / r, s, gr))
+    return out
 
 
 WORKLOADS = {"omni_128": omni_128, "omni_1024": omni_1024, "omni_4096": omni_4096}
