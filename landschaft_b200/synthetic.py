@@ -117,20 +117,46 @@ def omni_4096(seed: int = 0):
     return r, s, dict(radius=64, block_size=5, buffer=0, four_neighbors=False)
 
 
+def _advanced_draws(rng, side_min, side_max):
+    ny, nx = (int(v) for v in rng.integers(side_min, side_max + 1, 2))
+    r = np.exp(rng.uniform(np.log(1.0), np.log(1000.0), (ny, nx)))
+    a, b = rng.choice(ny * nx, 2, replace=False)
+    return ny, nx, r, int(a), int(b)
+
+
 def advanced_rasters(n=4096, seed=0, side_min=64, side_max=512):
     """(conductance, source, ground) triples of the advanced-mode batch."""
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(n):
-        ny, nx = (int(v) for v in rng.integers(side_min, side_max + 1, 2))
-        r = np.exp(rng.uniform(np.log(1.0), np.log(1000.0), (ny, nx)))
+        ny, nx, r, a, b = _advanced_draws(rng, side_min, side_max)
         s = np.zeros((ny, nx))
         gr = np.zeros((ny, nx))
-        a, b = rng.choice(ny * nx, 2, replace=False)
         s.flat[a] = 1.0
         gr.flat[b] = np.inf
         out.append((1.0 / r, s, gr))
     return out
+
+
+def advanced_packed(n=4096, seed=0, side_min=64, side_max=512):
+    """The same rasters as advanced_rasters, packed back to back: (shapes, conductance, source, ground)."""
+    rng = np.random.default_rng(seed)
+    shapes, gs, src, gnd = [], [], [], []
+    off = 0
+    for _ in range(n):
+        ny, nx, r, a, b = _advanced_draws(rng, side_min, side_max)
+        shapes.append((ny, nx))
+        gs.append((1.0 / r).ravel())
+        src.append(off + a)
+        gnd.append(off + b)
+        off += ny * nx
+    g = np.concatenate(gs)
+    del gs
+    s = np.zeros(off)
+    gr = np.zeros(off)
+    s[src] = 1.0
+    gr[gnd] = np.inf
+    return shapes, g, s, gr
 
 
 WORKLOADS = {"omni_128": omni_128, "omni_1024": omni_1024, "omni_4096": omni_4096}
