@@ -252,11 +252,17 @@ def bench_advanced(args, rank, world, local, d):
     source and one direct ground each, 4 neighbours; a step is one launch over the whole batch."""
     import torch
     from landschaft_b200 import raster, synthetic
-    shapes, g, s, gr = synthetic.advanced_packed(4096, seed=rank)
+    shapes, g, s, gr = synthetic.advanced_packed(64 if args.profile_run else 4096, seed=rank)
     n, cells = len(shapes), g.size
     dev = torch.device("cuda", local)
     gt, st, grt = (torch.from_numpy(x).to(dev) for x in (g, s, gr))
     p = raster.raster_params(four_neighbors=True)
+    if args.profile_run:
+        _, _, stats = raster.run_rasters(gt, st, grt, shapes, p)
+        print(json.dumps({"profile_run": "advanced_4096 (first 64 rasters)", "cells": int(cells),
+                          "cg_iterations_mean": stats.iters_total / max(stats.n_solved, 1)}), flush=True)
+        d.close()
+        return
     _, _, stats = raster.run_rasters(gt, st, grt, shapes, p)
     launches = int(__import__("landschaft_b200").omni.last_launch_count())
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
