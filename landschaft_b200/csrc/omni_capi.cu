@@ -194,7 +194,7 @@ ArenaLayout make_layout(const Variant &v, int H, int Wd, size_t smem_budget, boo
         size_t bytes;
     };
     std::vector<Item> items;  // in smem priority order
-    items.push_back({AR_ULIST, np * 4});
+    items.push_back({AR_ULIST, np * (raster ? 4 : 2)});  // u16 indices for windows, u32 for whole rasters
     items.push_back({AR_GT, np * ts});
     items.push_back({AR_P, np * ts});
     if (v.mg) items.push_back({AR_Z, np * ts});
@@ -737,7 +737,8 @@ int lsb_omniscape(const double *resistance, const double *source, int64_t nx, in
             static const char *names[PH_COUNT] = {"load", "flood", "mark", "assemble", "mg_setup", "resid64", "cg",
                                                   "vcycle", "currents", "other", "v_pre0", "v_restrict1",
                                                   "v_coarsest", "v_prolong0", "v_post0", "s_weights", "s_level1",
-                                                  "s_coarser", "s_dense", "ds1", "ds2+", "dr1", "dr2+", "up1",
+                                                  "s_coarser", "s_dense", "c_stage", "c_max", "ds1", "ds2+",
+                                                  "dr1", "dr2+", "up1",
                                                   "up2+", "us1", "us2+"};
             double tot = 0;
             for (int k = 0; k < PH_COUNT; ++k) tot += static_cast<double>(tm[k]);

@@ -29,6 +29,7 @@
 
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <math_constants.h>
 
 namespace lsb {
 
@@ -68,6 +69,26 @@ __device__ __forceinline__ double edge_w64(double a, double b, bool diag, bool s
     return diag ? (a + b) * kInvTwoSqrt2 : (a + b) * 0.5;
 }
 
+// The reference's test for leaving a branch current out of a node current, fabs(b / m) < 1e-8 (grid.cpp:19-71),
+// for one maximum m, decided by comparisons where that is unambiguous: the product 1e-8 m and the quotient b / m
+// round differently only within a relative 1e-15 or so of the threshold, so outside a band of 1e-6 around it the
+// decision is the same; inside it (and for a maximum that is not positive, finite and normal: empty band) the
+// quotient decides.
+struct Threshold {
+    double m, lo, hi;
+    __device__ explicit Threshold(double m_) : m(m_) {
+        const bool fast = m_ > 1e-290 && m_ < CUDART_INF;
+        lo = fast ? 1e-8 * m_ * (1.0 - 1e-6) : -1.0;
+        hi = fast ? 1e-8 * m_ * (1.0 + 1e-6) : -1.0;
+    }
+    __device__ __forceinline__ bool below(double b) const {
+        const double ab = fabs(b);
+        if (ab < lo) return true;
+        if (ab > hi && hi >= 0.0) return false;
+        return fabs(b / m) < 1e-8;
+    }
+};
+
 // d(edge weight)/d(first conductance); the weights are symmetric in their arguments.
 __device__ __forceinline__ double edge_dw64(double a, double b, bool diag, bool series) {
     if (series) {
@@ -102,7 +123,7 @@ constexpr int kNcMax = 25;     // cells of the coarsest level (solved by its den
 enum LevelArray : int { LV_C0 = 0, LV_CE, LV_CSW, LV_CS, LV_CSE, LV_INVD, LV_X, LV_B, LV_T, LV_COUNT };
 enum ArenaArray : int {
     AR_MASK = 0,  // u8
-    AR_ULIST,     // u32: padded indices of the unknowns, row-major
+    AR_ULIST,     // u16 (windows) or u32 (whole rasters): padded indices of the unknowns, row-major
     AR_G64,       // f64: conductance (-9999 outside / NoData; 0 on padding)
     AR_X64,       // f64: solution (potentials), 0 off the unknowns
     AR_B64,       // f64: scaled sources (the right-hand side)

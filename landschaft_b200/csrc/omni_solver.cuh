@@ -5,6 +5,8 @@
 
 #include <math_constants.h>
 
+#include <type_traits>
+
 #include "omni_device.cuh"
 
 namespace lsb {
@@ -59,6 +61,8 @@ enum Phase : int { PH_LOAD = 0, PH_FLOOD, PH_MARK, PH_ASSEMBLE, PH_MG_SETUP, PH_
                    PH_OTHER, PH_V_PRE0, PH_V_RESTRICT1, PH_V_COARSEST, PH_V_PROLONG0, PH_V_POST0,
                    // multigrid set-up: level-0 weights, level-1 Galerkin product, coarser products, coarsest inverse
                    PH_S_W, PH_S_L1, PH_S_LC, PH_S_DENSE,
+                   // node currents: staging the FP64 arrays, the branch maxima (the rest is PH_CURRENTS)
+                   PH_C_STAGE, PH_C_MAX,
                    // levels 1 and 2 (deeper levels count as 2): down smoothing, restriction; up prolongation, smoothing
                    PH_L_DS, PH_L_DR = PH_L_DS + 2, PH_L_UP = PH_L_DR + 2, PH_L_US = PH_L_UP + 2,
                    PH_COUNT = PH_L_US + 2 };
@@ -89,8 +93,8 @@ __device__ __forceinline__ double tmax(double a, double b) { return fmax(a, b); 
 
 // Block-wide ordered compaction of flags over [0, n): out[k] = i of the k-th
 // flagged i (increasing).  Returns the count.  scan: shared, >= 33 ints.
-template <int NT, typename F>
-__device__ __forceinline__ int block_compact(int n, F flag, uint32_t *out, int *scan) {
+template <int NT, typename I, typename F>
+__device__ __forceinline__ int block_compact(int n, F flag, I *out, int *scan) {
     constexpr int NW = NT / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int base = 0;
@@ -107,7 +111,7 @@ __device__ __forceinline__ int block_compact(int n, F flag, uint32_t *out, int *
             before += k < warp ? c : 0;
             total += c;
         }
-        if (f) out[base + before + __popc(m & ((1u << lane) - 1u))] = static_cast<uint32_t>(i);
+        if (f) out[base + before + __popc(m & ((1u << lane) - 1u))] = static_cast<I>(i);
         base += total;
         __syncthreads();
     }
@@ -129,6 +133,8 @@ __host__ __device__ constexpr bool hot_array(int k) {
 template <int NT, typename T, bool FOUR, bool MG, bool REFINE, bool HOT, bool ADV = false>
 struct Win {
     static_assert(REFINE || sizeof(T) == 8, "an FP32 inner solve needs the FP64 refinement");
+    // Padded indices of the unknowns: 16 bits for windows (below 65,536 padded cells), 32 for whole rasters.
+    using Idx = typename std::conditional<ADV, uint32_t, uint16_t>::type;
     using NB = Nb<FOUR>;
     static constexpr int ND = NB::ND, LOWER = NB::LOWER;
 
@@ -365,7 +371,7 @@ struct Win {
             mask[i] = m;
         }
         const double total = red.sum(t);
-        nu = block_compact<NT>(G.NP, [&](int i) { return (mask[i] & M_UNKNOWN) != 0; }, A<uint32_t>(AR_ULIST), scan);
+        nu = block_compact<NT, Idx>(G.NP, [&](int i) { return (mask[i] & M_UNKNOWN) != 0; }, A<Idx>(AR_ULIST), scan);
         return total;
     }
 
@@ -392,7 +398,7 @@ struct Win {
             if (ADV) A<T>(AR_FGT)[i] = static_cast<T>(A<double>(AR_FG64)[i]);
         }
         __syncthreads();
-        const uint32_t *ul = A<uint32_t>(AR_ULIST);
+        const Idx *ul = A<Idx>(AR_ULIST);
         for (int k = threadIdx.x; k < nu; k += NT) {
             const int i = ul[k];
             const double gi = g64[i];
@@ -424,7 +430,7 @@ struct Win {
     // the two cells' memory latencies overlap.
     template <class C, class Put>
     __device__ __forceinline__ void unknowns2(C calc, Put put) const {
-        const uint32_t *ul = A<uint32_t>(AR_ULIST);
+        const Idx *ul = A<Idx>(AR_ULIST);
         for (int k = threadIdx.x; k < nu; k += 2 * NT) {
             const bool two = k + NT < nu;
             const int i1 = ul[k], i2 = two ? ul[k + NT] : i1;
@@ -828,7 +834,7 @@ struct Win {
     // Also adds this thread's terms of r.z and r.r to rz and rr (its unknowns in increasing order), and copies z
     // to pcopy when given.
     __device__ __forceinline__ void vcycle(const T *r, double &rz, double &rr, T *pcopy = nullptr) {
-        const uint32_t *ul = A<uint32_t>(AR_ULIST);
+        const Idx *ul = A<Idx>(AR_ULIST);
         const T *gT = A<T>(AR_GT), *invd = A<T>(AR_INVD);
         T *z = A<T>(AR_Z), *q = A<T>(AR_Q);
         if (nlev == 1) {
@@ -1064,7 +1070,7 @@ struct Win {
     // most maxit iterations.
     // Returns the iterations; *ok = false on breakdown.
     __device__ __forceinline__ int pcg(T *d, T *r, double rtol, int maxit, bool use_mg, bool *ok) {
-        const uint32_t *ul = A<uint32_t>(AR_ULIST);
+        const Idx *ul = A<Idx>(AR_ULIST);
         const T *gT = A<T>(AR_GT), *invd = A<T>(AR_INVD);
         T *p = A<T>(AR_P), *q = A<T>(AR_Q);
         *ok = true;
@@ -1150,7 +1156,7 @@ struct Win {
     // reciprocal of 2 sqrt 2), stored as T in AR_R; returns (||r||^2, ||b||^2).
     __device__ __forceinline__ void residual64(double *rr_out, double *bb_out, bool first) {
         const uint8_t *mask = A<uint8_t>(AR_MASK);
-        const uint32_t *ul = A<uint32_t>(AR_ULIST);
+        const Idx *ul = A<Idx>(AR_ULIST);
         const double *g64 = A<double>(AR_G64), *x64 = A<double>(AR_X64), *b64 = A<double>(AR_B64);
         T *r = A<T>(AR_R);
         const bool series = a.series;
@@ -1195,7 +1201,7 @@ struct Win {
     // x64 must be zero on entry; with setup == false the multigrid hierarchy of the previous solve of the same
     // matrix is reused.
     __device__ __forceinline__ void solve(WinStat *st, bool setup = true) {
-        const uint32_t *ul = A<uint32_t>(AR_ULIST);
+        const Idx *ul = A<Idx>(AR_ULIST);
         double *x64 = A<double>(AR_X64);
         const bool want_mg = MG && a.sp.pc == 2;
         mark(PH_ASSEMBLE);
@@ -1338,6 +1344,7 @@ struct Win {
             }
         }
         red.max2(maxout, maxin);
+        const Threshold tin(maxin), tout(maxout);
         double J = 0.0, wabs = 0.0;
         for (int i = threadIdx.x; i < G.NP; i += NT) {
             const int py = row0(i), y = py - 1, x = i - py * G.P - 1;
@@ -1353,9 +1360,9 @@ struct Win {
                     if (!(mask[n] & M_PRESENT)) continue;
                     const double b = edge_w64(gi, g64[n], NB::diag(dd), series) * (v[n] - vi);
                     if (b > 0) {
-                        if (!(fabs(b / maxin) < 1e-8)) inflow += b;
+                        if (!tin.below(b)) inflow += b;
                     } else if (b < 0) {
-                        if (!(fabs(b / maxout) < 1e-8)) outflow -= b;
+                        if (!tout.below(b)) outflow -= b;
                     }
                 }
                 J += W * (inflow > outflow ? inflow : outflow);
@@ -1471,6 +1478,7 @@ struct Win {
                 vs[i] = v[i];
             }
             __syncthreads();
+            mark(PH_C_STAGE);
             currents_from(gs, vs, out, corr, cy0, cx0);
         } else {
             currents_from(g64, v, out, corr, cy0, cx0);
@@ -1496,9 +1504,11 @@ struct Win {
             }
         }
         red.max2(maxout, maxin);
+        mark(PH_C_MAX);
+        const Threshold tin(maxin), tout(maxout);
         const int W = a.W;
         for (int i = threadIdx.x; i < G.NP; i += NT) {
-            const int py = i / G.P, y = py - 1, x = i - py * G.P - 1;
+            const int py = row0(i), y = py - 1, x = i - py * G.P - 1;
             if (y < 0 || y >= G.h || x < 0 || x >= G.w) continue;
             double c = 0.0;
             if (mask[i] & M_PRESENT) {
@@ -1510,9 +1520,9 @@ struct Win {
                     if (!(mask[n] & M_PRESENT)) continue;
                     const double b = edge_w64(gi, g64[n], NB::diag(dd), series) * (v[n] - vi);
                     if (b > 0) {
-                        if (!(fabs(b / maxin) < 1e-8)) inflow += b;
+                        if (!tin.below(b)) inflow += b;
                     } else if (b < 0) {
-                        if (!(fabs(b / maxout) < 1e-8)) outflow -= b;
+                        if (!tout.below(b)) outflow -= b;
                     }
                 }
                 if (ADV) {
