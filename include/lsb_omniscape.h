@@ -84,7 +84,9 @@ typedef struct lsb_omni_params {
     int32_t preconditioner; /* lsb_preconditioner */
     double tol;             /* relative FP64 residual ||b - A x|| / ||b|| at which a window is solved */
     int32_t max_iter;       /* cap on CG iterations per window (all refinement steps together) */
-    int32_t threads_per_window; /* 0: chosen from the window size; else 256 or 512 */
+    int32_t threads_per_window; /* 0: chosen from the window size or the tuning table; else 128 (four windows per
+                                   SM, when a window's solver arrays fit a quarter of the SM's shared memory;
+                                   else 256), 256 or 512 */
     int32_t use_graph;      /* 1: capture the call's launches in a CUDA graph and replay it on repeat calls */
     int32_t mask_nodata;    /* 1: NaN on NoData cells of the outputs (Python's mask_nodata) */
 } lsb_omni_params;

@@ -161,14 +161,15 @@ Variant choose_variant(const lsb_omni_params *p, const Geom &g) {
     int pc = p->preconditioner;
     int nt = p->threads_per_window;
     TuneVal tv;
-    if ((pc == LSB_PC_AUTO || (nt != 256 && nt != 512)) && tune_lookup(p, g.W, &tv)) {
+    const auto valid_nt = [](int t) { return t == 128 || t == 256 || t == 512; };
+    if ((pc == LSB_PC_AUTO || !valid_nt(nt)) && tune_lookup(p, g.W, &tv)) {
         if (pc == LSB_PC_AUTO) pc = tv.pc;
-        if (nt != 256 && nt != 512) nt = tv.nt;
+        if (!valid_nt(nt)) nt = tv.nt;
     }
     if (pc == LSB_PC_AUTO) pc = v.dbl ? LSB_PC_JACOBI : LSB_PC_MG;
     v.pc = pc;
     v.mg = pc == LSB_PC_MG;
-    if (nt != 256 && nt != 512) {
+    if (!valid_nt(nt)) {
         const int np = (g.W + 2) * (g.W + 2);
         nt = np <= 1200 ? 256 : 512;
     }
@@ -257,6 +258,7 @@ ArenaLayout make_layout(const Variant &v, int H, int Wd, size_t smem_budget, boo
 // Kernel dispatch.
 // ---------------------------------------------------------------------------
 KernelFn pick(const Variant &v, bool hot) {
+    if (v.nt == 128) return pick_windows_128_hot(v.four, v.dbl, v.mg);  // (only with a shared-memory layout)
     if (v.nt == 256)
         return hot ? pick_windows_256_hot(v.four, v.dbl, v.mg) : pick_windows_256_gen(v.four, v.dbl, v.mg);
     return hot ? pick_windows_512_hot(v.four, v.dbl, v.mg) : pick_windows_512_gen(v.four, v.dbl, v.mg);
@@ -264,7 +266,7 @@ KernelFn pick(const Variant &v, bool hot) {
 
 struct DeviceInfo {
     int dev = -1, sms = 0;
-    size_t smem_optin = 0;
+    size_t smem_optin = 0, smem_sm = 0;
 };
 
 cudaError_t device_info(DeviceInfo *d) {
@@ -277,6 +279,9 @@ cudaError_t device_info(DeviceInfo *d) {
     e = cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->dev);
     if (e != cudaSuccess) return e;
     d->smem_optin = static_cast<size_t>(v);
+    e = cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, d->dev);
+    if (e != cudaSuccess) return e;
+    d->smem_sm = static_cast<size_t>(v);
     return cudaSuccess;
 }
 
@@ -312,7 +317,14 @@ int make_plan(int64_t nx, int64_t ny, const lsb_omni_params *p, Plan *pl, char *
     DeviceInfo di;
     LSB_CK(device_info(&di));
     const size_t budget = di.smem_optin > kStaticSmem ? di.smem_optin - kStaticSmem : 0;
-    pl->lay = make_layout(pl->v, g.W, g.W, budget, grad);
+    if (pl->v.nt == 128) {
+        // four windows per SM: each CTA gets a quarter of the SM's shared memory (less the per-CTA reserve); a
+        // window whose solver arrays do not fit runs on 256 threads instead
+        const size_t quarter = di.smem_sm / 4, reserve = 1024 + kStaticSmem;
+        pl->lay = make_layout(pl->v, g.W, g.W, quarter > reserve ? quarter - reserve : 0, grad);
+        if (!pl->lay.hot) pl->v.nt = 256;
+    }
+    if (pl->v.nt != 128) pl->lay = make_layout(pl->v, g.W, g.W, budget, grad);
     pl->kern = pick(pl->v, pl->lay.hot != 0);
     LSB_CK(cudaFuncSetAttribute(reinterpret_cast<const void *>(pl->kern),
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(pl->lay.smem_bytes)));
@@ -1160,7 +1172,7 @@ int lsb_rasters(int64_t n, const int32_t *nx, const int32_t *ny, const double *c
 int lsb_tune_set(int32_t window_width, int32_t four_neighbors, int32_t edge_weights, int32_t precision,
                  int32_t preconditioner, int32_t threads_per_window) {
     if (window_width < 1 || (preconditioner != LSB_PC_JACOBI && preconditioner != LSB_PC_MG) ||
-        (threads_per_window != 256 && threads_per_window != 512))
+        (threads_per_window != 128 && threads_per_window != 256 && threads_per_window != 512))
         return LSB_ERR_ARGUMENT;
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);

@@ -13,7 +13,7 @@ namespace lsb {
 // The persistent window solver.
 // ---------------------------------------------------------------------------
 template <int NT, typename T, bool FOUR, bool MG, bool REFINE, bool HOT>
-__global__ void __launch_bounds__(NT, 1) k_windows(const KArgs a) {
+__global__ void __launch_bounds__(NT, NT == 128 ? 4 : 1) k_windows(const KArgs a) {
     extern __shared__ __align__(16) char smem[];
     __shared__ double red_buf[128];
     __shared__ int scan_buf[64];
@@ -166,6 +166,7 @@ __global__ void __launch_bounds__(NT, 1) k_windows(const KArgs a) {
 
 
 // One translation unit per block size and layout kind instantiates the variants of that kind.
+KernelFn pick_windows_128_hot(bool four, bool dbl, bool mg);
 KernelFn pick_windows_256_hot(bool four, bool dbl, bool mg);
 KernelFn pick_windows_256_gen(bool four, bool dbl, bool mg);
 KernelFn pick_windows_512_hot(bool four, bool dbl, bool mg);

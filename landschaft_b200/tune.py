@@ -6,9 +6,11 @@ installs the fastest in the library's tuning table (``lsb_tune_set``).  Calls th
 ``"auto"`` and the threads per window on 0 then use it.  The table is process-wide; ``save_tuning`` and
 ``load_tuning`` keep it in a JSON file.
 
-The candidates: multigrid V(1,1) or Jacobi preconditioning, with 256 or 512 threads per window (one window per
-CTA, one persistent CTA per SM).  Timing is the device time of the window kernels (CUDA events around them), the
-best of ``repeats`` runs after one warm-up run, on a centred crop of the rasters holding about ``windows`` targets.
+The candidates: multigrid V(1,1) or Jacobi preconditioning, with 512 or 256 threads per window (one window per
+CTA, one persistent CTA per SM) or 128 (one window per CTA, four CTAs per SM: for small windows; a window too large
+for a quarter of the SM's shared memory runs on 256).  Timing is the device time of the window kernels (CUDA events
+around them), the best of ``repeats`` runs after one warm-up run, on a centred crop of the rasters holding about
+``windows`` targets.
 """
 
 from __future__ import annotations
@@ -21,7 +23,7 @@ import numpy as np
 from . import _native as N
 from .omni import EDGE_WEIGHTS, PRECONDITIONERS, active_blocks, make_params, run_device
 
-CANDIDATES = (("mg", 512), ("mg", 256), ("jacobi", 512), ("jacobi", 256))
+CANDIDATES = (("mg", 512), ("mg", 256), ("mg", 128), ("jacobi", 512), ("jacobi", 256), ("jacobi", 128))
 
 _TABLE: dict[tuple, dict] = {}  # mirror of the library's table: key -> entry
 

@@ -27,7 +27,7 @@ def test_autotune_installs_the_fastest_candidate(lsb):
     lsb.clear_tuning()
     entry = lsb.autotune(r, s, kw["radius"], block_size=1, windows=400)
     times = {k: v for k, v in entry["window_ms"].items() if v is not None}
-    assert set(entry["window_ms"]) == {"mg/512", "mg/256", "jacobi/512", "jacobi/256"}
+    assert set(entry["window_ms"]) == {"mg/512", "mg/256", "mg/128", "jacobi/512", "jacobi/256", "jacobi/128"}
     best = f'{entry["preconditioner"]}/{entry["threads_per_window"]}'
     assert times[best] == min(times.values())
     pc, nt = C.c_int32(), C.c_int32()
