@@ -201,7 +201,8 @@ typedef struct lsb_raster_params {
     int32_t precision;      /* lsb_precision: FP32 CG + FP64 refinement (multigrid) or FP64 CG (Jacobi) */
     double tol;             /* relative FP64 residual at which a component is solved */
     int32_t max_iter;       /* cap on CG iterations per component */
-    int32_t pad_;
+    int32_t smem_limit_kb;  /* shared memory per CTA for solver arrays, KiB (0: all there is); what is left over is
+                               L1 cache for the arrays in global memory */
     double memory_limit;    /* bytes of solver scratch in global memory (0: 8 GiB); fewer CTAs when exceeded */
 } lsb_raster_params;
 

@@ -52,7 +52,7 @@ class Stats(C.Structure):
 
 class RasterParams(C.Structure):
     _fields_ = [("four_neighbors", C.c_int32), ("precision", C.c_int32), ("tol", C.c_double),
-                ("max_iter", C.c_int32), ("pad_", C.c_int32), ("memory_limit", C.c_double)]
+                ("max_iter", C.c_int32), ("smem_limit_kb", C.c_int32), ("memory_limit", C.c_double)]
 
 
 class NativeError(RuntimeError):

@@ -583,7 +583,8 @@ int raster_plan(int64_t n, const int32_t *nx, const int32_t *ny, const lsb_raste
     v.nt = 512;
     DeviceInfo di;
     LSB_CK(device_info(&di));
-    const size_t budget = di.smem_optin > kStaticSmem ? di.smem_optin - kStaticSmem : 0;
+    size_t budget = di.smem_optin > kStaticSmem ? di.smem_optin - kStaticSmem : 0;
+    if (p->smem_limit_kb > 0) budget = std::min<size_t>(budget, static_cast<size_t>(p->smem_limit_kb) << 10);
     pl->lay = make_layout(v, H, Wd, budget, false, true);
     pl->kern = pick_rasters(pl->lay.hot != 0, v.four, v.dbl);
     LSB_CK(cudaFuncSetAttribute(reinterpret_cast<const void *>(pl->kern),

@@ -45,7 +45,7 @@ def _inputs(conductance, source, ground):
 
 
 def raster_params(four_neighbors=False, solver="fp32-refine", tol=1e-12, max_iter=20000,
-                  memory_limit=0.0) -> N.RasterParams:
+                  memory_limit=0.0, smem_limit_kb=0) -> N.RasterParams:
     if solver not in SOLVERS:
         raise ValueError(f"solver must be one of {SOLVERS}")
     p = N.default_raster_params()
@@ -54,6 +54,7 @@ def raster_params(four_neighbors=False, solver="fp32-refine", tol=1e-12, max_ite
     p.tol = float(tol)
     p.max_iter = int(max_iter)
     p.memory_limit = float(memory_limit or 0.0)
+    p.smem_limit_kb = int(smem_limit_kb)
     return p
 
 
