@@ -197,11 +197,12 @@ ArenaLayout make_layout(const Variant &v, int H, int Wd, size_t smem_budget, boo
     std::vector<Item> items;  // in smem priority order
     items.push_back({AR_ULIST, np * (raster ? 4 : 2)});  // u16 indices for windows, u32 for whole rasters
     items.push_back({AR_GT, np * ts});
+    items.push_back({AR_R, np * ts});
+    items.push_back({AR_INVD, np * ts});
+    // P, Z, Q, D adjacent: between inner solves they are dead and hold the FP64 residual's staged copies
     items.push_back({AR_P, np * ts});
     if (v.mg) items.push_back({AR_Z, np * ts});
     items.push_back({AR_Q, np * ts});
-    items.push_back({AR_R, np * ts});
-    items.push_back({AR_INVD, np * ts});
     const bool has_d = !(v.dbl && !v.refine);
     if (has_d) items.push_back({AR_D, np * ts});
     if (v.mg) {
@@ -247,7 +248,15 @@ ArenaLayout make_layout(const Variant &v, int H, int Wd, size_t smem_budget, boo
     // scratch, the span from the stencil conductances to the mask (solver vectors, levels, coarsest inverse: dead
     // by then) holds copies of both if it is large enough
     L.stage = kNoStage;
+    L.rstage = kNoStage;
     const bool g_global = (L.off[AR_G64] & 0x80000000u) || (L.off[AR_X64] & 0x80000000u);
+    if (L.hot && g_global) {
+        // the span of P, Z, Q, D (consecutive items, all in shared memory when hot)
+        size_t span = 0;
+        for (const Item &it : items)
+            if (it.arr == AR_P || it.arr == AR_Z || it.arr == AR_Q || it.arr == AR_D) span += align_up(it.bytes, 16);
+        if (span >= 2 * np * 8) L.rstage = L.off[AR_P];
+    }
     if (L.hot && g_global && !(L.off[AR_MASK] & 0x80000000u) && L.off[AR_MASK] > L.off[AR_GT] &&
         L.off[AR_MASK] - L.off[AR_GT] >= 2 * np * 8)
         L.stage = L.off[AR_GT];

@@ -153,6 +153,7 @@ struct ArenaLayout {
     uint32_t gmem_bytes;  // per CTA
     uint32_t hot;         // 1: every array but the FP64 window arrays is in shared memory
     uint32_t stage;       // shared offset of 2 x (h+2)(w+2) doubles free during the node currents, or kNoStage
+    uint32_t rstage;      // the same, free between inner solves (the FP64 residual), or kNoStage
 };
 
 // Solver configuration for one launch.

@@ -1154,10 +1154,56 @@ struct Win {
 
     // r = b - A x in FP64 over the unknowns (exact weights up to the
     // reciprocal of 2 sqrt 2), stored as T in AR_R; returns (||r||^2, ||b||^2).
+    // Copies the NP doubles of a and b (global scratch) to as and bs (shared memory), then a barrier.  Each thread
+    // issues all its loads of a round before its stores, so that the loads' latencies overlap (the compiler cannot
+    // reorder them past the stores itself: it cannot tell the pointers apart).
+    __device__ __forceinline__ void stage2(const double *a, const double *b, double *as, double *bs) {
+        constexpr int K = 4;
+        for (int i0 = threadIdx.x; i0 < G.NP; i0 += K * NT) {
+            double va[K], vb[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const int i = i0 + k * NT;
+                va[k] = i < G.NP ? a[i] : 0.0;
+                vb[k] = i < G.NP ? b[i] : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const int i = i0 + k * NT;
+                if (i < G.NP) {
+                    as[i] = va[k];
+                    bs[i] = vb[k];
+                }
+            }
+        }
+        __syncthreads();
+    }
+
     __device__ __forceinline__ void residual64(double *rr_out, double *bb_out, bool first) {
+        if (HOT && !first && a.lay.rstage != kNoStage) {
+            // the FP64 conductance and solution live in global scratch and the CG vectors P, Z, Q, D are dead
+            // between inner solves: both are copied into them first, so that the stencil reads are on chip
+            double *gs = reinterpret_cast<double *>(sm + a.lay.rstage), *xs = gs + G.NP;
+            stage2(A<double>(AR_G64), A<double>(AR_X64), gs, xs);
+            residual64_from(gs, xs, rr_out, bb_out, false);  // ends with a barrier
+            // the CG and the V-cycle read P, Z and Q at cells next to the unknowns: zero again
+            T *p = A<T>(AR_P), *q = A<T>(AR_Q), *z = A<T>(AR_Z);
+            for (int i = threadIdx.x; i < G.NP; i += NT) {
+                p[i] = T(0);
+                q[i] = T(0);
+                if (MG) z[i] = T(0);
+            }
+            __syncthreads();
+        } else {
+            residual64_from(A<double>(AR_G64), A<double>(AR_X64), rr_out, bb_out, first);
+        }
+    }
+
+    __device__ __forceinline__ void residual64_from(const double *g64, const double *x64, double *rr_out,
+                                                    double *bb_out, bool first) {
         const uint8_t *mask = A<uint8_t>(AR_MASK);
         const Idx *ul = A<Idx>(AR_ULIST);
-        const double *g64 = A<double>(AR_G64), *x64 = A<double>(AR_X64), *b64 = A<double>(AR_B64);
+        const double *b64 = A<double>(AR_B64);
         T *r = A<T>(AR_R);
         const bool series = a.series;
         double rr = 0.0, bb = 0.0;
@@ -1473,11 +1519,7 @@ struct Win {
             // the FP64 conductance and potentials live in global scratch; the solver's vectors and levels are
             // dead now, so both are copied into that shared memory first (then every stencil read is on chip)
             double *gs = reinterpret_cast<double *>(sm + a.lay.stage), *vs = gs + G.NP;
-            for (int i = threadIdx.x; i < G.NP; i += NT) {
-                gs[i] = g64[i];
-                vs[i] = v[i];
-            }
-            __syncthreads();
+            stage2(g64, v, gs, vs);
             mark(PH_C_STAGE);
             currents_from(gs, vs, out, corr, cy0, cx0);
         } else {
