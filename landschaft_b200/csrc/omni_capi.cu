@@ -388,6 +388,7 @@ SolveParams solve_params(const lsb_omni_params *p, int pc) {
     sp.max_outer = 12;
     sp.pc = pc;
     sp.omega = 0.9f;
+    sp.omega_c = 0.7f;
     return sp;
 }
 

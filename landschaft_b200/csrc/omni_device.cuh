@@ -163,7 +163,8 @@ struct SolveParams {
     int max_iter;      // cap on CG iterations (all refinement steps)
     int max_outer;     // cap on refinement steps
     int pc;            // 1 Jacobi, 2 multigrid
-    float omega;       // damped-Jacobi smoothing weight
+    float omega;       // damped-Jacobi smoothing weight on the fine level (safe below 1: lambda_max(D^-1 A) <= 2)
+    float omega_c;     // the same on the Galerkin coarse levels, which have no such bound
 };
 
 // Per-solve statistics written by the kernel.

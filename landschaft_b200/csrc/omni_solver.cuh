@@ -720,7 +720,7 @@ struct Win {
                 t[J] = T(0);
             }
             __syncthreads();
-            const T om = static_cast<T>(a.sp.omega);
+            const T om = static_cast<T>(a.sp.omega_c);
             for_cells(l, [&](int jy, int jx, int J) {
                 T acc[5] = {T(0), T(0), T(0), T(0), T(0)};
                 bool act = false;
@@ -1333,7 +1333,11 @@ struct Win {
                 __syncthreads();
                 bool ok = true;
                 const int budget = a.sp.max_iter - iters;
-                const int it = pcg(d, r, a.sp.inner_tol, budget < 1 ? 1 : budget, use_mg, &ok);
+                // a multigrid-preconditioned step that needs more than kMgSteps iterations for its 1e-4 has a
+                // preconditioner that fails on this window: the stall test below then switches to Jacobi
+                constexpr int kMgSteps = 200;
+                const int cap = use_mg && budget > kMgSteps ? kMgSteps : budget;
+                const int it = pcg(d, r, a.sp.inner_tol, cap < 1 ? 1 : cap, use_mg, &ok);
                 iters += it;
                 ++outer;
                 for (int k = threadIdx.x; k < nu; k += NT) {
