@@ -453,7 +453,8 @@ def main():
     peak, peak_kind = peaks()
     achieved = hbm_bytes / ktime / 1e9
     prof = ROOT / "profiles" / "k_windows_omni_1024_traffic.json"
-    traffic = json.loads(prof.read_text())["dram_bytes_per_launch"] if prof.exists() and not args.crop else None
+    traffic = (json.loads(prof.read_text())["dram_bytes_per_launch"]
+               if prof.exists() and not args.crop and args.workload == "omni_1024" else None)
     smem_bytes = kstats.unknown_iters * 84.0  # per unknown and CG iteration (FP32, 8 neighbours)
     smem_peak = SMEM_BYTES_PER_CYCLE * SMS * (clk["sm_mhz"] or 1965.0) * 1e6 / 1e9
 
