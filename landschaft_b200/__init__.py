@@ -19,5 +19,6 @@ from .omni import (  # noqa: F401
 from .autograd import grad_device, omniscape_current  # noqa: F401,E402
 from .tune import autotune, clear_tuning, load_tuning, save_tuning, tuning_table  # noqa: F401,E402
 from .raster import AdvancedResult, advanced, advanced_batch  # noqa: F401,E402
+from .ini import omniscape_ini, parse_ini, read_ascii_grid, write_ascii_grid  # noqa: F401,E402
 
 __version__ = "0.1.0"

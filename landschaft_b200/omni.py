@@ -165,6 +165,11 @@ class Dataset:
     def __contains__(self, key):
         return key in self._vars
 
+    def __setitem__(self, key, value):
+        """``ds[name] = values`` or ``ds[name] = (dims, values)``, as xarray takes a new map."""
+        values = value[1] if isinstance(value, tuple) else value
+        self._vars[key] = Variable(key, np.asarray(values))
+
     def __iter__(self):
         return iter(self._vars)
 

@@ -6,9 +6,13 @@ landschaft source tree).  Reads the reference's own test data:
 * ``tests/data/reference/circuit/omniscape.npz``: 8 Omniscape.jl 0.7 runs
   (inputs, options and the CHOLMOD outputs; the cg+amg outputs are left out);
 * ``tests/data/reference/circuit/advanced.npz`` + ``advanced_inputs.npz``: 6
-  Circuitscape advanced-mode solves (CHOLMOD node currents).
+  Circuitscape advanced-mode solves (CHOLMOD node currents);
+* ``tests/data/reference/circuit/omniscape_ini/*.ini``, ``omniscape_input/*``
+  (ASCII grids and a reclass table) and ``omniscape_ini.npz``: 11 Omniscape.jl
+  INI runs (the CHOLMOD outputs; the cg+amg outputs are left out).
 
-Writes ``omniscape_golden.npz`` and ``advanced_golden.npz`` next to this file.
+Writes ``omniscape_golden.npz``, ``advanced_golden.npz``, ``omniscape_ini.npz``
+and copies of the INI and input files (same layout) next to this file.
 The GPU machines do not have the reference tree, so the tests read only these
 fixtures.
 """
@@ -40,6 +44,12 @@ def main():
     out = {k: inp[k] for k in inp.files}
     out.update({k: ref[k] for k in ref.files if k.endswith("current_cholmod")})
     np.savez_compressed(HERE / "advanced_golden.npz", **out)
+    z = np.load(data / "omniscape_ini.npz")
+    np.savez_compressed(HERE / "omniscape_ini.npz", **{k: z[k] for k in z.files if "/cgamg/" not in k})
+    for sub in ("omniscape_ini", "omniscape_input"):
+        (HERE / sub).mkdir(exist_ok=True)
+        for f in sorted((data / sub).iterdir()):
+            (HERE / sub / f.name).write_bytes(f.read_bytes())
 
 
 if __name__ == "__main__":
