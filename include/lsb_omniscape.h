@@ -89,6 +89,14 @@ typedef struct lsb_omni_params {
                                    else 256), 256 or 512 */
     int32_t use_graph;      /* 1: capture the call's launches in a CUDA graph and replay it on repeat calls */
     int32_t mask_nodata;    /* 1: NaN on NoData cells of the outputs (Python's mask_nodata) */
+    /* Streaming (no counterpart in the reference, which streams inside one call): solve only the targets
+     * target_begin <= t < target_end of the target order (target_end 0: to the last), adding their currents to
+     * the outputs' values when accumulate is 1 (else the outputs start at 0).  The maps of consecutive ranges,
+     * each call continuing the previous one's outputs, are bitwise those of one call; the normalised current and
+     * the NoData mask are applied by the call whose range reaches the last target. */
+    int32_t accumulate;
+    int64_t target_begin;
+    int64_t target_end;
 } lsb_omni_params;
 
 typedef struct lsb_omni_stats {

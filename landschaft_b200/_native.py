@@ -36,7 +36,8 @@ class Params(C.Structure):
                 ("condition1", Condition), ("condition2", Condition), ("memory_limit", C.c_double),
                 ("precision", C.c_int32), ("preconditioner", C.c_int32), ("tol", C.c_double),
                 ("max_iter", C.c_int32), ("threads_per_window", C.c_int32), ("use_graph", C.c_int32),
-                ("mask_nodata", C.c_int32)]
+                ("mask_nodata", C.c_int32), ("accumulate", C.c_int32), ("target_begin", C.c_int64),
+                ("target_end", C.c_int64)]
 
 
 class Stats(C.Structure):

@@ -422,8 +422,10 @@ int enqueue(const Plan &pl, const double *res, const double *src, const lsb_omni
     const Geom &g = pl.g;
     const int64_t n = g.nx * g.ny;
     int64_t launches = 0;
-    LSB_CK(cudaMemsetAsync(cur, 0, n * 8, s));
-    if (g.fp) LSB_CK(cudaMemsetAsync(fpm, 0, n * 8, s));
+    if (!p->accumulate) {
+        LSB_CK(cudaMemsetAsync(cur, 0, n * 8, s));
+        if (g.fp) LSB_CK(cudaMemsetAsync(fpm, 0, n * 8, s));
+    }
     LSB_CK(cudaMemsetAsync(ws + pl.o_count, 0, 4, s));
     LSB_CK(cudaMemsetAsync(ws + pl.o_queue, 0, (pl.nbatches + 1) * 4, s));
     LSB_CK(cudaMemsetAsync(ws + pl.o_err, 0, 4, s));
@@ -507,10 +509,14 @@ int enqueue(const Plan &pl, const double *res, const double *src, const lsb_omni
     a.fp_win = g.fp ? reinterpret_cast<double *>(ws + pl.o_fp) : nullptr;
     a.stat = stat;
     a.batch_size = static_cast<int>(pl.batch);
+    const int64_t t0 = std::max<int64_t>(p->target_begin, 0);
+    const int64_t t1 = p->target_end > 0 ? std::min<int64_t>(p->target_end, g.NL) : g.NL;
+    a.target_end = p->target_end > 0 ? static_cast<int>(t1) : 0;
+    const int nb = t1 > t0 ? static_cast<int>((t1 - t0 + pl.batch - 1) / pl.batch) : 0;
     const dim3 gg(static_cast<unsigned>((g.nx + kGatherTX - 1) / kGatherTX),
                   static_cast<unsigned>((g.ny + kGatherTY - 1) / kGatherTY));
-    for (int b = 0; b < pl.nbatches && g.NL > 0; ++b) {
-        a.batch_start = static_cast<int>(b * pl.batch);
+    for (int b = 0; b < nb && g.NL > 0; ++b) {
+        a.batch_start = static_cast<int>(t0 + b * pl.batch);
         a.queue = queue + b;
         if (ev) LSB_CK(cudaEventRecord(ev[2 * b], s));
         pl.kern<<<pl.grid, pl.v.nt, pl.lay.smem_bytes, s>>>(a);
@@ -519,7 +525,7 @@ int enqueue(const Plan &pl, const double *res, const double *src, const lsb_omni
         launches += 2;
         LSB_CK(cudaGetLastError());
     }
-    if (norm || p->mask_nodata) {
+    if ((norm || p->mask_nodata) && p->target_end <= 0) {
         k_finish<<<static_cast<int>((n + 255) / 256), 256, 0, s>>>(res, n, cur, g.fp ? fpm : nullptr, norm,
                                                                   p->mask_nodata);
         ++launches;

@@ -236,7 +236,8 @@ __global__ void __launch_bounds__(kGatherTX *kGatherTY) k_gather(const KArgs a, 
     const int64_t X0 = static_cast<int64_t>(blockIdx.x) * kGatherTX, Y0 = static_cast<int64_t>(blockIdx.y) * kGatherTY;
     const int64_t X = X0 + (threadIdx.x % kGatherTX), Y = Y0 + (threadIdx.x / kGatherTX);
     const bool in = X < a.nx && Y < a.ny;
-    const int n_batch = min(*a.count_ptr - a.batch_start, a.batch_size);
+    const int last = (a.target_end > 0 && a.target_end < *a.count_ptr) ? a.target_end : *a.count_ptr;
+    const int n_batch = min(last - a.batch_start, a.batch_size);
     if (n_batch <= 0) return;
     const int D = a.D, bs = a.bs, br = a.br, W = a.W;
     const int64_t X1 = X0 + kGatherTX - 1, Y1 = Y0 + kGatherTY - 1;

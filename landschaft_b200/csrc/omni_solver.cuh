@@ -35,6 +35,7 @@ struct KArgs {
     WinStat *stat;    // per target: [land, flow]
     int *queue;       // work counter of this launch
     int batch_start, batch_size;
+    int target_end;   // > 0: targets from target_end on are left out (a streamed range)
     // working memory
     char *gscratch;   // gridDim.x slices of lay.gmem_bytes
     ArenaLayout lay;

@@ -53,7 +53,8 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 4 : 1) k_windows(const KArgs a
     if (a.mode == 1) {
         count = 2;
     } else {
-        count = *a.count_ptr - a.batch_start;
+        const int last = (a.target_end > 0 && a.target_end < *a.count_ptr) ? a.target_end : *a.count_ptr;
+        count = last - a.batch_start;
         if (count > a.batch_size) count = a.batch_size;
     }
     const int W = a.W, D = a.D;

@@ -335,6 +335,87 @@ def run_device(r, s, params: N.Params, *, normalized=False, out=None, want_stats
         return out, stats
 
 
+def _fingerprint(r, s, params: N.Params) -> str:
+    """Identifies a run for its checkpoint: the rasters and every parameter but the streaming fields."""
+    import hashlib
+    p = N.Params.from_buffer_copy(params)
+    p.accumulate, p.target_begin, p.target_end, p.use_graph = 0, 0, 0, 0
+    p.condition1.present = p.condition1.future = p.condition2.present = p.condition2.future = None
+    h = hashlib.sha1(bytes(p))
+    for t in (r, s):
+        h.update(t.detach().cpu().numpy().tobytes())
+    return h.hexdigest()
+
+
+def run_device_streamed(r, s, params: N.Params, *, chunk_windows: int, checkpoint=None, normalized=False,
+                        max_chunks=None):
+    """``run_device`` in consecutive ranges of ``chunk_windows`` targets, each continuing the previous one's maps
+    (bitwise the maps of one call), with a checkpoint after every range.
+
+    ``checkpoint``: an ``.npz`` file; when it exists and belongs to the same rasters and parameters, the run resumes
+    after its last range (a finished run's file returns its maps at once).  ``max_chunks``: stop after that many
+    ranges (the checkpoint then holds the partial maps; the returned stats are None).  Returns
+    ``(outputs, stats)`` as ``run_device``, the stats summed over the ranges.
+    """
+    import os
+    from pathlib import Path
+    import torch
+    ny, nx = r.shape
+    total = int(active_blocks(s.detach().cpu().numpy(), params.block_size).sum())
+    key = _fingerprint(r, s, params)
+    out = {"current": torch.zeros((ny, nx), dtype=torch.float64, device=r.device)}
+    if params.flow_potential:
+        out["flow_potential"] = torch.zeros_like(out["current"])
+    if normalized:
+        out["normalized"] = torch.zeros_like(out["current"])
+    fields = ("n_solved", "n_failed", "iters_total", "iters_max", "refine_max", "worst_residual", "unknown_iters")
+    agg = dict.fromkeys(fields, 0)
+    begin, done = 0, False
+    ck = Path(checkpoint) if checkpoint is not None else None
+    if ck is not None and ck.exists():
+        z = np.load(ck)
+        if str(z["key"]) != key:
+            raise ValueError(f"the checkpoint {ck} belongs to another run (other rasters or parameters)")
+        for name, t in out.items():
+            if name in z.files:
+                t.copy_(torch.from_numpy(z[name]))
+        begin, done = int(z["next_target"]), bool(z["done"])
+        agg.update({k: z[k].item() for k in fields})
+
+    def save(finished):
+        if ck is None:
+            return
+        tmp = ck.with_name(ck.name + ".tmp.npz")
+        np.savez(tmp, key=key, next_target=begin, done=finished, **{k: v.cpu().numpy() for k, v in out.items()},
+                 **{k: np.array(v) for k, v in agg.items()})
+        os.replace(tmp, ck)
+
+    p = N.Params.from_buffer_copy(params)
+    p.use_graph = 0
+    p.accumulate = 1
+    chunks = 0
+    while not done:
+        end = begin + max(int(chunk_windows), 1)
+        last = end >= total
+        p.target_begin = begin
+        p.target_end = 0 if last else end
+        _, st = run_device(r, s, p, normalized=normalized and last, out=out)
+        for k in ("n_solved", "n_failed", "iters_total", "unknown_iters"):
+            agg[k] += getattr(st, k)
+        for k in ("iters_max", "refine_max", "worst_residual"):
+            agg[k] = max(agg[k], getattr(st, k))
+        begin, done = (total if last else end), last
+        chunks += 1
+        save(done)
+        if not done and max_chunks is not None and chunks >= max_chunks:
+            return out, None
+    stats = N.Stats()
+    stats.n_targets = total
+    for k, v in agg.items():
+        setattr(stats, k, v)
+    return out, stats
+
+
 def last_launch_count() -> int:
     """Kernels the last call on this thread launched (a graph replay: the graph's kernel nodes)."""
     return int(N.load().lsb_last_launch_count())
@@ -413,7 +494,8 @@ def omniscape(resistance, radius, *, source=None, block_size=1, buffer=0, source
               condition1_upper: float = 0.0, condition2_lower: float = 0.0, condition2_upper: float = 0.0,
               precision: str = "double", memory_limit: float | None = None, n_threads: int = 0,
               solver: str = "fp32-refine", preconditioner: str = "auto", edge_weights: str = "average",
-              tol: float = 1e-12, device=None, return_stats: bool = False):
+              tol: float = 1e-12, device=None, return_stats: bool = False, checkpoint=None,
+              chunk_windows: int | None = None):
     """Omnidirectional connectivity with Omniscape's moving-window circuits, solved on one GPU.
 
     Arguments, defaults and results are those of landschaft's ``ls.omniscape``
@@ -428,7 +510,9 @@ def omniscape(resistance, radius, *, source=None, block_size=1, buffer=0, source
     FP64 iterative refinement; ``"fp64"``: FP64 CG), ``preconditioner``
     (``"auto"``, ``"jacobi"``, ``"mg"``), ``edge_weights`` (``"average"``, as
     Omniscape; ``"series"``: resistor-series weights), ``tol`` (relative FP64
-    residual of every window solve), ``device``, ``return_stats``.
+    residual of every window solve), ``device``, ``return_stats``, and streaming with resume: ``chunk_windows``
+    solves the targets in consecutive ranges of that many windows (bitwise the same maps), ``checkpoint`` (an
+    ``.npz`` path) saves the partial maps after every range and resumes from them.
     ``n_threads`` is accepted and has no effect; ``memory_limit`` bounds the
     device memory of one batch of window buffers.
 
@@ -512,7 +596,11 @@ def omniscape(resistance, radius, *, source=None, block_size=1, buffer=0, source
     params = make_params(radius, buffer, block_size, four_neighbors, resistance_is_conductance, correct_artifacts,
                          compute_fp, edge_weights, solver, preconditioner, tol, mask_nodata=mask_nodata,
                          memory_limit=memory_limit or 0.0, conditions=dcond or None)
-    out, stats = run_device(rt, stt, params, normalized=bool(normalized_current))
+    if chunk_windows or checkpoint is not None:
+        out, stats = run_device_streamed(rt, stt, params, chunk_windows=int(chunk_windows or 100000),
+                                         checkpoint=checkpoint, normalized=bool(normalized_current))
+    else:
+        out, stats = run_device(rt, stt, params, normalized=bool(normalized_current))
     cum = out["current"].cpu().numpy()
     data = {"cum_currmap": cum}
     if compute_fp:
