@@ -243,6 +243,47 @@ void lsb_tune_clear(void);
 /* Library version string. */
 const char *lsb_version(void);
 
+/* ---- Circuitscape pairwise solves on a node graph ----------------------------------------------------------------
+ * Replace, for one connected component, the factorisation and the batched back substitutions of
+ * circuit::raster_pairwise (src/cpp/circuit/circuitscape.cpp:587-660, factor_component :93-141) and the node
+ * currents of graph_node_currents (circuitscape.cpp:38-77).  The component has n nodes in CSR form: ptr[n + 1]
+ * (int64), adj (int32, ascending within a row, local node numbers in the graph's order), w (edge conductances,
+ * >= 0) and diag (the Laplacian's diagonal: the row's conductances summed, plus the shift of the reference's
+ * factorisation).  Node `ground` is held at 0 V.  Job j draws a unit current from node src[j] and injects it at
+ * dst[j] (either may be the ground); volt[j n + i] = v_i - v_src[j] (the voltages relative to the source, the
+ * reference's per-pair voltages), and cur[j n + i] (when cur != NULL) = max(inflow, outflow) at node i, branch
+ * currents under 1e-8 of the largest in- / outflow left out.  One CTA solves a job at a time (FP64 CG with Jacobi
+ * preconditioning and true-residual restarts).  All pointers but stats and err are device pointers. */
+typedef struct lsb_graph_params {
+    double tol;        /* target relative residual ||b - A x|| / ||b|| (default 1e-14); the solve also stops when
+                          the true residual stops decreasing */
+    double accept;     /* a job whose final relative residual exceeds this fails (default 1e-9) */
+    int32_t max_iter;  /* cap on CG iterations per job (0: 20 n + 2000) */
+    int32_t max_ctas;  /* persistent CTAs (0: 4 per SM, fewer when the scratch exceeds 8 GiB) */
+} lsb_graph_params;
+
+typedef struct lsb_graph_stats {
+    int64_t jobs;
+    int64_t failures;       /* jobs above `accept` or out of iterations */
+    int32_t iters_max;
+    int32_t ctas;           /* CTAs launched */
+    double iters_mean;
+    double worst_residual;  /* largest final relative residual */
+} lsb_graph_stats;
+
+/* Defaults: tol 1e-14, accept 1e-9, max_iter 0, max_ctas 0. */
+void lsb_graph_params_default(lsb_graph_params *p);
+
+/* Device bytes lsb_graph_pairs needs. */
+int lsb_graph_pairs_workspace_size(int64_t n, int64_t n_jobs, const lsb_graph_params *p, size_t *bytes);
+
+/* Solves the jobs on `stream`.  With stats != NULL the call waits for the stream, fills the statistics and returns
+ * LSB_ERR_NOT_CONVERGED when a job failed. */
+int lsb_graph_pairs(int64_t n, const int64_t *ptr, const int32_t *adj, const double *w, const double *diag,
+                    int32_t ground, int64_t n_jobs, const int32_t *src, const int32_t *dst,
+                    const lsb_graph_params *p, double *volt, double *cur, void *workspace, size_t workspace_bytes,
+                    lsb_graph_stats *stats, char *err, size_t errlen, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -21,7 +21,8 @@ EDGE_AVERAGE, EDGE_SERIES = 0, 1
 EXPORTS = ("lsb_params_default", "lsb_omniscape_workspace_size", "lsb_omniscape", "lsb_omniscape_correction",
            "lsb_omniscape_grad", "lsb_omniscape_grad_workspace_size", "lsb_last_launch_count",
            "lsb_time_window_kernels", "lsb_version", "lsb_omniscape_noalloc", "lsb_tune_set", "lsb_tune_get",
-           "lsb_tune_clear", "lsb_raster_params_default", "lsb_rasters_workspace_size", "lsb_rasters")
+           "lsb_tune_clear", "lsb_raster_params_default", "lsb_rasters_workspace_size", "lsb_rasters",
+           "lsb_graph_params_default", "lsb_graph_pairs_workspace_size", "lsb_graph_pairs")
 
 
 class Condition(C.Structure):
@@ -54,6 +55,15 @@ class Stats(C.Structure):
 class RasterParams(C.Structure):
     _fields_ = [("four_neighbors", C.c_int32), ("precision", C.c_int32), ("tol", C.c_double),
                 ("max_iter", C.c_int32), ("smem_limit_kb", C.c_int32), ("memory_limit", C.c_double)]
+
+
+class GraphParams(C.Structure):
+    _fields_ = [("tol", C.c_double), ("accept", C.c_double), ("max_iter", C.c_int32), ("max_ctas", C.c_int32)]
+
+
+class GraphStats(C.Structure):
+    _fields_ = [("jobs", C.c_int64), ("failures", C.c_int64), ("iters_max", C.c_int32), ("ctas", C.c_int32),
+                ("iters_mean", C.c_double), ("worst_residual", C.c_double)]
 
 
 class NativeError(RuntimeError):
@@ -115,6 +125,13 @@ def load():
         lib.lsb_rasters.argtypes = [i64, vp, vp, vp, vp, vp, C.POINTER(RasterParams), vp, vp, vp, sz,
                                     C.POINTER(Stats), C.c_char_p, sz, vp]
         lib.lsb_rasters.restype = C.c_int
+        lib.lsb_graph_params_default.argtypes = [C.POINTER(GraphParams)]
+        lib.lsb_graph_params_default.restype = None
+        lib.lsb_graph_pairs_workspace_size.argtypes = [i64, i64, C.POINTER(GraphParams), C.POINTER(sz)]
+        lib.lsb_graph_pairs_workspace_size.restype = C.c_int
+        lib.lsb_graph_pairs.argtypes = [i64, vp, vp, vp, vp, i32, i64, vp, vp, C.POINTER(GraphParams), vp, vp, vp,
+                                        sz, C.POINTER(GraphStats), C.c_char_p, sz, vp]
+        lib.lsb_graph_pairs.restype = C.c_int
         _lib = lib
         return lib
 
@@ -128,6 +145,12 @@ def default_params() -> Params:
 def default_raster_params() -> RasterParams:
     p = RasterParams()
     load().lsb_raster_params_default(C.byref(p))
+    return p
+
+
+def default_graph_params() -> GraphParams:
+    p = GraphParams()
+    load().lsb_graph_params_default(C.byref(p))
     return p
 
 

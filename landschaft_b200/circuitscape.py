@@ -1,0 +1,835 @@
+"""Circuitscape's pairwise mode on rasters (``ls.circuit.circuitscape_pairwise``) with its solves on the GPU.
+
+Mirrors ``src/landschaft/circuit/circuitscape.py`` (the readers :30-330, ``circuitscape_pairwise`` :550-670 and the
+pairwise branch of ``circuitscape_ini`` :1039-1213) and the native ``circuit::raster_graph`` /
+``circuit::raster_pairwise`` (``src/cpp/circuit/circuitscape.cpp:145-263,474-743``).  The node graph is built on
+the host with numpy, as the reference builds it on the host in C++; the solves and the node currents run on the GPU
+through ``lsb_graph_pairs`` of the C ABI: one CTA per pair solves the component's grounded Laplacian (CSR) by FP64
+Jacobi-preconditioned CG and computes the pair's node currents; the reference factorises each component once
+(CHOLMOD-like multifrontal Cholesky) and back-substitutes every pair.
+
+Scope: single-cell focal points (raster or text list), short-circuit polygons, masks, include/exclude pair files,
+reclass tables, and every pairwise map option.  Focal regions (several cells sharing an id, the reference's
+``raster_pairwise_regions``), GeoTIFF inputs and the other scenarios raise ``NotImplementedError``.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import gzip
+import math
+import os
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+from . import _native as N
+
+NODATA = -9999.0
+TRUELIST = ("True", "true", "1")
+FALSELIST = ("False", "false", "0")
+K_SHIFT = 10 * np.finfo(np.float64).eps  # added to the Laplacian's diagonal, as the reference's factorisation does
+SQRT2 = 1.4142135623730951
+TWO_SQRT2 = 2 * SQRT2
+
+
+# --- readers (circuitscape.py:30-330) -----------------------------------------------------------------------------
+
+@dataclass
+class RasterMeta:
+    nrows: int
+    ncols: int
+    xllcorner: float
+    yllcorner: float
+    cellsize: float
+
+
+def _open(path):
+    p = os.fspath(path)
+    return gzip.open(p, "rt") if p.lower().endswith("gz") else open(p, encoding="utf-8")
+
+
+def file_type(path) -> str:
+    """``geotiff``, ``npy``, ``aagrid``, ``pairs_aagrid``, ``pairs`` or ``list`` (circuitscape.py:48-70)."""
+    p = os.fspath(path)
+    with (gzip.open if p.lower().endswith("gz") else open)(p, "rb") as f:
+        head = f.read(4)
+    if head[2:4] == b"\x2a\x00":
+        return "geotiff"
+    with _open(p) as f:
+        line = f.readline()
+    if line.startswith("\x93NUMPY"):
+        return "npy"
+    if line.lower().startswith("ncols"):
+        return "aagrid"
+    if line.startswith("min"):
+        return "pairs_aagrid"
+    if line.startswith("mode"):
+        return "pairs"
+    return "list"
+
+
+_ASC_KEYS = ("ncols", "nrows", "xllcorner", "yllcorner", "xllcenter", "yllcenter", "cellsize", "dx", "dy",
+             "nodata_value")
+
+
+def read_raster(path):
+    """An ESRI ASCII grid (optionally gzipped) parsed in double, NoData and NaN set to -9999
+    (circuitscape.py:73-124).  Returns ``(values, RasterMeta)``."""
+    p = os.fspath(path)
+    if not os.path.isfile(p):
+        raise FileNotFoundError(f'the file "{p}" does not exist')
+    if not p.lower().removesuffix(".gz").endswith(".asc"):
+        raise NotImplementedError(f"{p}: only ESRI ASCII grids are read (no GeoTIFF reader in this package)")
+    header: dict[str, float] = {}
+    rows = []
+    with _open(p) as f:
+        for line in f:
+            toks = line.split()
+            if not toks:
+                continue
+            if not rows and len(toks) == 2 and toks[0].lower() in _ASC_KEYS:
+                header[toks[0].lower()] = float(toks[1])
+                continue
+            rows.append([float(t) for t in toks])
+    nrows, ncols = int(header["nrows"]), int(header["ncols"])
+    a = np.array(rows, dtype=np.float64)
+    if a.shape != (nrows, ncols):
+        raise ValueError(f"{p}: the ASCII grid does not hold {nrows} rows of {ncols} values")
+    dx = header.get("dx", header.get("cellsize", math.nan))
+    dy = header.get("dy", dx)
+    xll = header["xllcorner"] if "xllcorner" in header else header["xllcenter"] - dx / 2
+    yll = header["yllcorner"] if "yllcorner" in header else header["yllcenter"] - dy / 2
+    nodata = header.get("nodata_value", NODATA)
+    a[(a == nodata) | np.isnan(a)] = NODATA
+    return a, RasterMeta(nrows, ncols, xll, yll, dx)
+
+
+def _read_rows(path) -> list:
+    with _open(path) as f:
+        return [[float(t) for t in line.split()] for line in f if line.split()]
+
+
+def _list_cells(points: np.ndarray, meta: RasterMeta):
+    # 1-based row and column: ceil(nrows - (y - yll) / cellsize), ceil((x - xll) / cellsize)
+    i = np.ceil(meta.nrows - (points[:, 2] - meta.yllcorner) / meta.cellsize).astype(np.int64)
+    j = np.ceil((points[:, 1] - meta.xllcorner) / meta.cellsize).astype(np.int64)
+    return i, j
+
+
+def read_polymap(path, habitat: RasterMeta, *, integer: bool = False, nodata_as=0.0) -> np.ndarray:
+    """A raster on the habitat's grid with NoData set to ``nodata_as`` (circuitscape.py:151-160)."""
+    a, meta = read_raster(path)
+    if integer and not np.all(a == np.round(a)):
+        raise ValueError(f"{path} contains non-integer values")
+    if nodata_as is not None:
+        a[a == NODATA] = nodata_as
+    if (meta.nrows, meta.ncols) != (habitat.nrows, habitat.ncols):
+        raise ValueError(f"{path} is not on the habitat's grid")
+    return a
+
+
+@dataclass
+class FocalPoints:
+    """Focal points: 1-based rows, columns and ids, sorted by id; cells sharing an id form a focal region."""
+
+    rows: np.ndarray
+    cols: np.ndarray
+    ids: np.ndarray
+
+    @property
+    def cells(self):
+        return np.asarray(self.rows) - 1, np.asarray(self.cols) - 1
+
+    @property
+    def has_regions(self) -> bool:
+        return len(self.ids) != len(np.unique(self.ids))
+
+
+def _sorted_points(i, j, v) -> FocalPoints:
+    keep = v >= 0
+    i, j, v = i[keep], j[keep], v[keep]
+    order = np.argsort(v, kind="stable")
+    return FocalPoints(i[order].astype(np.int64), j[order].astype(np.int64), v[order].astype(np.int64))
+
+
+def read_point_map(path, habitat: RasterMeta) -> FocalPoints:
+    """A raster of ids or a text list of ``id x y``; negative ids dropped, sorted by id (circuitscape.py:209-229)."""
+    if file_type(path) == "list":
+        pts = np.array(_read_rows(path), dtype=np.float64).reshape(-1, 3)
+        i, j = _list_cells(pts, habitat)
+        fp = _sorted_points(i, j, pts[:, 0])
+    else:
+        a = read_polymap(path, habitat, integer=True)
+        jj, ii = np.nonzero(a.T)  # column-major order
+        fp = _sorted_points(ii + 1, jj + 1, a[ii, jj])
+    i, j, v = fp.rows, fp.cols, fp.ids
+    if len(v) and (i.min() < 0 or j.min() < 0 or i.max() > habitat.nrows or j.max() > habitat.ncols):
+        raise ValueError("At least one focal node location falls outside of habitat map")
+    if len(np.unique(v)) < 2:
+        raise ValueError("Less than two valid focal nodes found. Please check focal node location file.")
+    return fp
+
+
+@dataclass
+class IncludedPairs:
+    """Include / exclude pairs: ``mode`` ("include" or "exclude"), the ids and a 0/1 matrix over them."""
+
+    mode: str
+    ids: np.ndarray
+    matrix: np.ndarray
+
+    def excluded(self) -> set:
+        target = 0 if self.mode == "include" else 1
+        m, n = self.matrix, len(self.ids)
+        return {(int(self.ids[i]), int(self.ids[j])) for j in range(n) for i in range(n)
+                if m[i, j] == target and m[j, i] == target}
+
+
+def read_included_pairs(path) -> IncludedPairs:
+    """A ``min``/``max`` matrix or a ``mode`` list of pairs (circuitscape.py:283-311)."""
+    kind = file_type(path)
+    with _open(path) as f:
+        lines = f.read().splitlines()
+    if kind == "pairs_aagrid":
+        minval, maxval = float(lines[0].split()[1]), float(lines[1].split()[1])
+        a = np.array([[float(t) for t in ln.split()] for ln in lines[2:] if ln.split()])
+        ids = a[0, 1:].astype(np.int64)
+        m = a[1:, 1:]
+        m = np.where(m > maxval, 0, m)
+        return IncludedPairs("include", ids, (m >= minval).astype(np.int64))
+    if kind == "pairs":
+        mode = lines[0].split()[1]
+        pairs = np.array([[float(t) for t in ln.split()] for ln in lines[1:] if ln.split()]).reshape(-1, 2)
+        ids = np.unique(pairs).astype(np.int64)
+        ids = ids[ids != 0]
+        pos = {int(v): k for k, v in enumerate(ids)}
+        m = np.zeros((len(ids), len(ids)), dtype=np.int64)
+        for a, b in pairs.astype(np.int64):
+            if a in pos and b in pos:
+                m[pos[a], pos[b]] = m[pos[b], pos[a]] = 1
+        return IncludedPairs(mode, ids, m)
+    raise ValueError("Error reading focal node include/exclude pairs file.")
+
+
+def read_reclass_table(path) -> dict:
+    t = np.array(_read_rows(path), dtype=np.float64)
+    if t.ndim != 2 or t.shape[1] != 2:
+        raise ValueError(f"{path} must have exactly 2 columns")
+    return {float(a): float(b) for a, b in t}
+
+
+def habitat_conductance(cells, *, is_resistance: bool = True, reclass: dict | None = None) -> np.ndarray:
+    """Optionally reclassified, then 1 / resistance (or the conductance), -9999 cells at 0
+    (circuitscape.py:329-348)."""
+    c = np.array(cells, dtype=np.float64)
+    if reclass:
+        flat = c.ravel()
+        for k, v in enumerate(flat):
+            if v in reclass:
+                flat[k] = reclass[v]
+        c = flat.reshape(c.shape)
+    nodata = c == NODATA
+    if is_resistance:
+        if np.any(c == 0):
+            raise ValueError("zero resistance values are not supported for habitat maps; use a short-circuit "
+                             "region file instead")
+        g = 1 / c
+    else:
+        g = c.copy()
+    g[nodata] = 0.0
+    return g
+
+
+# --- the node graph (circuitscape.cpp:145-263) ----------------------------------------------------------------------
+
+@dataclass
+class RasterGraph:
+    """Nodes: habitat cells numbered column-major, the cells of a short-circuit region with habitat merged into
+    the node of its first habitat cell.  CSR adjacency (neighbours ascending) with the summed edge conductances,
+    the Laplacian's diagonal and the connected components (numbered by their smallest node)."""
+
+    nx: int
+    ny: int
+    n_nodes: int
+    nodemap: np.ndarray   # cell (row-major) -> node, -1: none
+    ptr: np.ndarray       # int64, n_nodes + 1
+    adj: np.ndarray       # int32
+    w: np.ndarray         # float64
+    degree: np.ndarray    # float64
+    comp: np.ndarray      # node -> component
+    n_comp: int
+
+
+def _average(x, y, diagonal: bool, resistances: bool):
+    if resistances:
+        with np.errstate(divide="ignore"):
+            s = (1 / x + 1 / y) / 2
+            return 1 / (SQRT2 * s) if diagonal else 1 / s
+    return (x + y) / TWO_SQRT2 if diagonal else (x + y) / 2
+
+
+def raster_graph(gmap: np.ndarray, polymap: np.ndarray | None, avg_resistances: bool,
+                 four_neighbors: bool) -> RasterGraph:
+    ny, nx = gmap.shape
+    n = nx * ny
+    g = np.ascontiguousarray(gmap, dtype=np.float64).ravel()
+    cm = np.arange(n).reshape(ny, nx).T.ravel()  # cells in column-major order
+    hab_cm = cm[g[cm] > 0]
+    label = np.zeros(n, dtype=np.int64)
+    label[hab_cm] = np.arange(1, len(hab_cm) + 1)
+    if polymap is not None:
+        pm = np.ascontiguousarray(polymap, dtype=np.int64).ravel()
+        sel = hab_cm[pm[hab_cm] != 0]
+        ids, first = np.unique(pm[sel], return_index=True)  # first habitat cell of each region, column-major
+        first_label = label[sel[first]]
+        cells = np.flatnonzero(pm != 0)
+        k = np.searchsorted(ids, pm[cells])
+        k_ok = k < len(ids)
+        hit = np.zeros(len(cells), dtype=bool)
+        hit[k_ok] = ids[k[k_ok]] == pm[cells[k_ok]]
+        label[cells[hit]] = first_label[k[hit]]
+    on = label != 0
+    uniq, inv = np.unique(label[on], return_inverse=True)
+    nodemap = np.full(n, -1, dtype=np.int64)
+    nodemap[on] = inv
+    n_nodes = len(uniq)
+
+    # edges in column-major cell order: right, below, below right, above right; both orientations
+    ys, xs = np.divmod(cm, nx)
+    dirs = [(xs + 1 < nx, 1, False), (ys + 1 < ny, nx, False)]
+    if not four_neighbors:
+        dirs += [((ys + 1 < ny) & (xs + 1 < nx), nx + 1, True), ((ys > 0) & (xs + 1 < nx), 1 - nx, True)]
+    rank_of = np.empty(n, dtype=np.int64)
+    rank_of[cm] = np.arange(n)  # position of each cell in column-major order
+    A, B, W, order = [], [], [], []
+    for d, (ok, off, diag) in enumerate(dirs):
+        c = cm[ok & (nodemap[cm] >= 0)]
+        e = c + off
+        a, b = nodemap[c], nodemap[e]
+        keep = b >= 0
+        c, e, a, b = c[keep], e[keep], a[keep], b[keep]
+        w = _average(g[c], g[e], diag, avg_resistances)
+        keep = a != b  # within a merged node: nothing in the Laplacian
+        c, a, b, w = c[keep], a[keep], b[keep], w[keep]
+        rank = rank_of[c]
+        for first, (p, q) in enumerate(((a, b), (b, a))):
+            A.append(p)
+            B.append(q)
+            W.append(w)
+            order.append((rank * 4 + d) * 2 + first)
+    A, B, W, order = (np.concatenate(x) if x else np.zeros(0) for x in (A, B, W, order))
+    o = np.argsort(order, kind="stable")
+    A, B, W = A[o].astype(np.int64), B[o].astype(np.int64), W[o]
+    s = np.lexsort((B, A))  # stable: duplicates keep the order met
+    A, B, W = A[s], B[s], W[s]
+    if len(A):
+        start = np.flatnonzero(np.r_[True, (A[1:] != A[:-1]) | (B[1:] != B[:-1])])
+        wsum = W[start].copy()
+        dup = np.diff(np.r_[start, len(A)]) > 1
+        for k in np.flatnonzero(dup):  # duplicates (merged nodes) summed in the order met
+            acc = W[start[k]]
+            for t in range(start[k] + 1, start[k + 1] if k + 1 < len(start) else len(A)):
+                acc = acc + W[t]
+            wsum[k] = acc
+        A, B = A[start], B[start]
+    else:
+        wsum = W
+    ptr = np.zeros(n_nodes + 1, dtype=np.int64)
+    np.add.at(ptr, A + 1, 1)
+    ptr = np.cumsum(ptr)
+    degree = np.zeros(n_nodes)
+    # the diagonal sums each row's entries in adjacency order
+    for k in range(int(np.diff(ptr).max()) if n_nodes and len(A) else 0):
+        rows = np.flatnonzero(ptr[:-1] + k < ptr[1:])
+        degree[rows] += wsum[ptr[:-1][rows] + k]
+    comp, n_comp = _components(n_nodes, ptr, B, wsum)
+    return RasterGraph(nx, ny, n_nodes, nodemap, ptr, B.astype(np.int32), wsum.astype(np.float64), degree, comp,
+                       n_comp)
+
+
+def _components(n_nodes, ptr, adj, w):
+    """Connected components over the edges of nonzero weight, numbered by their smallest node."""
+    from scipy.sparse import csr_matrix
+    from scipy.sparse.csgraph import connected_components
+    if n_nodes == 0:
+        return np.zeros(0, dtype=np.int64), 0
+    rows = np.repeat(np.arange(n_nodes), np.diff(ptr))
+    nz = w != 0  # edges of weight 0 do not connect (stored zeros would count as edges)
+    m = csr_matrix((np.ones(int(nz.sum()), dtype=np.int8), (rows[nz], np.asarray(adj)[nz])),
+                   shape=(n_nodes, n_nodes))
+    k, lab = connected_components(m, directed=False)
+    _, first = np.unique(lab, return_index=True)
+    rank = np.empty(k, dtype=np.int64)
+    rank[np.argsort(first)] = np.arange(k)
+    return rank[lab], int(k)
+
+
+# --- the GPU solves -------------------------------------------------------------------------------------------------
+
+@dataclass
+class GraphSolveStats:
+    jobs: int = 0
+    iters_max: int = 0
+    iters_mean: float = 0.0
+    failures: int = 0
+
+
+def _solve_component(graph: RasterGraph, members: np.ndarray, ground: int, src: np.ndarray, dst: np.ndarray,
+                     want_currents: bool, params, stats: GraphSolveStats, device):
+    """Every job (src, dst node) on one component: unit current into dst, out of src, the ground node at 0 V.
+    Returns (volt, cur) as numpy arrays of jobs x members: the voltages relative to the source node, and the node
+    currents (None without ``want_currents``)."""
+    import torch
+    lib = N.load()
+    m = len(members)
+    local = np.full(graph.n_nodes, -1, dtype=np.int64)
+    local[members] = np.arange(m)
+    lens = graph.ptr[members + 1] - graph.ptr[members]
+    idx = np.repeat(graph.ptr[members], lens) + (np.arange(lens.sum()) - np.repeat(np.cumsum(lens) - lens, lens))
+    la = local[graph.adj[idx]]
+    keep = la >= 0  # edges leaving the component carry no conductance
+    rowid = np.repeat(np.arange(m), lens)[keep]
+    ptr = np.zeros(m + 1, dtype=np.int64)
+    np.add.at(ptr, rowid + 1, 1)
+    ptr = np.cumsum(ptr)
+    adj = la[keep].astype(np.int32)
+    w = graph.w[idx][keep]
+    diag = graph.degree[members] + K_SHIFT
+    dev = device
+    t = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).to(dev)  # noqa: E731
+    d_ptr, d_adj, d_w, d_diag = t(ptr, np.int64), t(adj, np.int32), t(w, np.float64), t(diag, np.float64)
+    js, jd = local[src].astype(np.int32), local[dst].astype(np.int32)
+    nj = len(js)
+    volt = np.empty((nj, m))
+    cur = np.empty((nj, m)) if want_currents else None
+    # jobs in batches of bounded output size
+    per = max(1, min(nj, (1 << 27) // max(m * 16, 1)))
+    for b0 in range(0, nj, per):
+        b1 = min(nj, b0 + per)
+        nb = b1 - b0
+        d_src, d_dst = t(js[b0:b1], np.int32), t(jd[b0:b1], np.int32)
+        d_v = torch.empty((nb, m), dtype=torch.float64, device=dev)
+        d_c = torch.empty((nb, m), dtype=torch.float64, device=dev) if want_currents else None
+        nbytes = C.c_size_t(0)
+        rc = lib.lsb_graph_pairs_workspace_size(m, nb, C.byref(params), C.byref(nbytes))
+        N.check(rc, C.create_string_buffer(b"invalid graph size or parameters"))
+        ws = torch.empty(max(int(nbytes.value), 16), dtype=torch.uint8, device=dev)
+        st = N.GraphStats()
+        err = C.create_string_buffer(1024)
+        stream = torch.cuda.current_stream(dev)
+        rc = lib.lsb_graph_pairs(m, d_ptr.data_ptr(), d_adj.data_ptr(), d_w.data_ptr(), d_diag.data_ptr(),
+                                 int(local[ground]), nb, d_src.data_ptr(), d_dst.data_ptr(), C.byref(params),
+                                 d_v.data_ptr(), d_c.data_ptr() if d_c is not None else None, ws.data_ptr(),
+                                 ws.numel(), C.byref(st), err, len(err), stream.cuda_stream)
+        N.check(rc, err)
+        volt[b0:b1] = d_v.cpu().numpy()
+        if want_currents:
+            cur[b0:b1] = d_c.cpu().numpy()
+        stats.iters_mean = (stats.iters_mean * stats.jobs + st.iters_mean * nb) / (stats.jobs + nb)
+        stats.jobs += nb
+        stats.iters_max = max(stats.iters_max, int(st.iters_max))
+        stats.failures += int(st.failures)
+    if stats.failures:
+        raise N.NativeError(f"{stats.failures} pair solves did not converge")
+    return volt, cur
+
+
+def graph_params(tol=1e-13, max_iter=0):
+    p = N.default_graph_params()
+    p.tol = float(tol)
+    if max_iter:
+        p.max_iter = int(max_iter)
+    return p
+
+
+# --- pairwise (circuitscape.cpp:474-743) ----------------------------------------------------------------------------
+
+@dataclass
+class PairOptions:
+    volt_maps: bool = False
+    cur_maps: bool = False
+    cum: bool = False
+    max: bool = False
+    focal_zero: bool = False
+    null_currents: bool = False
+    null_voltages: bool = False
+    log_transform: bool = False
+
+    def maps(self) -> bool:
+        return self.volt_maps or self.cur_maps or self.cum or self.max
+
+
+def raster_pairwise(graph: RasterGraph, gmap: np.ndarray, points: np.ndarray, excluded: np.ndarray,
+                    o: PairOptions, emit=None, *, tol=1e-13, device=None, stats: GraphSolveStats | None = None):
+    """Effective resistances between the focal points' nodes ``points`` (-1: off the graph), with the pair maps.
+
+    Returns ``(resistances n x n, cum, max)``; ``emit(ci, cj, voltage_map, current_map)`` receives each pair's maps
+    (None where not asked for).  Follows circuitscape.cpp:474-743: components in order, distinct focal nodes in
+    first-appearance order, the component's last node grounded, jobs (source, destination) solved with a unit
+    current, and without maps or exclusions the shortcut (only the first focal node's pairs, the others from the
+    voltages)."""
+    import torch
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    params = graph_params(tol)
+    stats = stats if stats is not None else GraphSolveStats()
+    npt = len(points)
+    ncell = graph.nx * graph.ny
+    gflat = np.ascontiguousarray(gmap, dtype=np.float64).ravel()
+    R = np.full((npt, npt), -1.0)
+    shortcut = not o.maps() and not excluded.any()
+    voltmatrix = np.zeros((npt, npt)) if shortcut else None
+    short_res = np.full((npt, npt), -1.0) if shortcut else None
+    cum = np.zeros(ncell) if o.cum else None
+    mx = np.full(ncell, NODATA) if o.max else None
+    order = np.argsort(graph.comp, kind="stable")
+    bounds = np.searchsorted(graph.comp[order], np.arange(graph.n_comp + 1))
+    positions: dict[int, list] = {}
+    for i, v in enumerate(points):
+        if v >= 0:
+            positions.setdefault(int(v), []).append(i)
+    comp_of = np.append(graph.comp, -1)  # index -1 (no node) gives component -1
+    pcomp = comp_of[np.asarray(points, dtype=np.int64)]
+    cell_comp = comp_of[graph.nodemap]
+    for k in range(graph.n_comp):
+        csub = []
+        for i in range(npt):
+            v = int(points[i])
+            if v >= 0 and pcomp[i] == k and v not in csub:
+                csub.append(v)
+        if not csub:
+            continue
+        for v in csub:
+            pos = positions[v]
+            for a in range(len(pos)):
+                for b in range(a + 1, len(pos)):
+                    R[pos[a], pos[b]] = R[pos[b], pos[a]] = 0.0
+        nsrc = min(1, len(csub)) if shortcut else len(csub)
+        jobs = [(csub[si], csub[di]) for si in range(nsrc) for di in range(si + 1, len(csub))
+                if any(not excluded[ci, cj] for ci in positions[csub[si]] for cj in positions[csub[di]])]
+        if not jobs:
+            continue
+        members = order[bounds[k]:bounds[k + 1]]  # ascending (stable sort of ascending nodes)
+        ground = int(members[-1])
+        src = np.array([j[0] for j in jobs], dtype=np.int64)
+        dst = np.array([j[1] for j in jobs], dtype=np.int64)
+        volt, cur = _solve_component(graph, members, ground, src, dst, o.maps(), params, stats, dev)
+        mindex = {int(v): q for q, v in enumerate(members)}
+        in_k = cell_comp == k
+        cells_k = np.flatnonzero(in_k)
+        node_q = np.searchsorted(members, graph.nodemap[cells_k])
+        for jn, (s, d) in enumerate(jobs):
+            vcol = volt[jn]
+            resistance = vcol[mindex[d]] - vcol[mindex[s]]
+            vmap = cmap = None
+            if o.maps():
+                if o.volt_maps:
+                    vmap = np.zeros(ncell)
+                    vmap[cells_k] = vcol[node_q]
+                    if o.null_voltages:
+                        vmap[gflat == 0] = NODATA
+                cmap = np.zeros(ncell)
+                cmap[cells_k] = cur[jn][node_q]
+                if o.focal_zero:
+                    nodes_k = graph.nodemap[cells_k]
+                    cmap[cells_k[(nodes_k == s) | (nodes_k == d)]] = 0.0
+                if o.log_transform:
+                    with np.errstate(divide="ignore", invalid="ignore"):
+                        cmap = np.where(cmap > 0, np.log10(np.where(cmap > 0, cmap, 1.0)), NODATA)
+                if o.null_currents:
+                    cmap[gflat == 0] = NODATA
+            for ci in positions[s]:
+                for cj in positions[d]:
+                    if excluded[ci, cj]:
+                        continue
+                    R[ci, cj] = R[cj, ci] = resistance
+                    if shortcut:
+                        for i in range(1, npt):
+                            v = int(points[i])
+                            if v < 0 or pcomp[i] != k:
+                                continue
+                            voltmatrix[i, cj] = 1 - vcol[mindex[v]] / resistance
+                        continue
+                    if not o.maps():
+                        continue
+                    if o.cum:
+                        cum += cmap
+                    if o.max:
+                        np.maximum(mx, cmap, out=mx)
+                    if emit is not None and (o.volt_maps or o.cur_maps):
+                        emit(ci, cj, vmap.reshape(graph.ny, graph.nx) if vmap is not None else None,
+                             cmap.reshape(graph.ny, graph.nx).copy() if o.cur_maps else None)
+        if shortcut:
+            _shortcut(R, short_res, voltmatrix, points, pcomp, k, positions[csub[0]][0])
+    if shortcut:
+        R = short_res
+    np.fill_diagonal(R, 0.0)
+    if cum is not None:
+        cum = np.maximum(cum, NODATA).reshape(graph.ny, graph.nx)
+    if mx is not None:
+        mx = np.maximum(mx, NODATA).reshape(graph.ny, graph.nx)
+    return R, cum, mx
+
+
+def _shortcut(R, S, voltmatrix, points, pcomp, k, anchor):
+    """The resistances of every pair of the component from those of its anchor's pairs and the voltages
+    (circuitscape.cpp:705-731)."""
+    invalid = -777.0
+    npt = len(points)
+    check = [points[i] >= 0 and pcomp[i] == k for i in range(npt)]
+    for x in range(npt):
+        if not check[x]:
+            continue
+        r1x = R[anchor, x]
+        if r1x == -1:
+            continue
+        S[x, anchor] = S[anchor, x] = r1x
+        for y in range(x, npt):
+            if not check[y]:
+                continue
+            r12 = R[anchor, y]
+            if r12 == -1:
+                continue
+            if r1x != invalid:
+                S[anchor, y] = S[y, anchor] = r12
+                r2x = 2 * r12 * voltmatrix[x, y] + r1x - r12
+                if S[y, x] != invalid:
+                    S[y, x] = S[x, y] = r2x
+            else:
+                S[x, :] = invalid
+                S[:, x] = invalid
+
+
+# --- the public calls ------------------------------------------------------------------------------------------------
+
+@dataclass
+class CircuitscapeResult:
+    """``resistances``: ids in the first row and column (-1: not connected); ``cum_current``, ``max_current``:
+    sum and maximum of the pairs' current maps; ``maps``: per-pair maps."""
+
+    resistances: np.ndarray | None = None
+    cum_current: np.ndarray | None = None
+    max_current: np.ndarray | None = None
+    maps: dict = field(default_factory=dict)
+    stats: GraphSolveStats | None = None
+
+
+def _grid(value, name) -> np.ndarray:
+    a = np.array(value, dtype=np.float64)
+    if a.ndim != 2:
+        raise ValueError(f"{name} must be a 2-D raster")
+    return np.where(np.isnan(a), NODATA, a)
+
+
+def _points_from_map(pm: np.ndarray) -> FocalPoints:
+    pm = pm.copy()
+    pm[pm == NODATA] = 0
+    jj, ii = np.nonzero(pm.T)
+    return _sorted_points(ii + 1, jj + 1, pm[ii, jj])
+
+
+def _apply_included_pairs(points: FocalPoints, pairs: IncludedPairs | None):
+    if pairs is None:
+        return points, set()
+    if pairs.mode == "include":
+        keep = np.isin(points.ids, pairs.ids)
+        points = FocalPoints(points.rows[keep], points.cols[keep], points.ids[keep])
+    return points, pairs.excluded()
+
+
+def _run_pairwise(g, poly, points: FocalPoints, excluded_ids: set, four, avg, o: PairOptions, emit, tol, device):
+    if points.has_regions:
+        raise NotImplementedError("focal regions (several cells per focal id) are not supported")
+    graph = raster_graph(g, poly, avg, four)
+    rows, cols = points.cells
+    cells = rows * g.shape[1] + cols
+    ok = (cells >= 0) & (cells < g.size)
+    nodes = np.where(ok, graph.nodemap[np.where(ok, cells, 0)], -1)
+    ids = points.ids
+    n = len(ids)
+    ex = np.zeros((n, n), dtype=bool)
+    if excluded_ids:
+        for a in range(n):
+            for b in range(n):
+                ex[a, b] = (int(ids[a]), int(ids[b])) in excluded_ids
+    stats = GraphSolveStats()
+    R, cum, mx = raster_pairwise(graph, g, nodes, ex, o, emit, tol=tol, device=device, stats=stats)
+    res = np.zeros((n + 1, n + 1))
+    res[0, 1:] = ids
+    res[1:, 0] = ids
+    res[1:, 1:] = R
+    return res, cum, mx, stats
+
+
+def circuitscape_pairwise(habitat, points, *, habitat_is_resistance: bool = True, polygons=None, mask=None,
+                          four_neighbors: bool = False, avg_resistances: bool = False, included_pairs=None,
+                          voltage_maps: bool = False, current_maps: bool = False, cum_map: bool = False,
+                          max_map: bool = False, set_focal_node_currents_to_zero: bool = False,
+                          set_null_currents_to_nodata: bool = False, set_null_voltages_to_nodata: bool = False,
+                          log_transform_maps: bool = False, reclass: dict | None = None, n_threads: int = 0,
+                          tol: float = 1e-13, device=None) -> CircuitscapeResult:
+    """Effective resistances between every pair of focal points on a raster (drop-in for
+    ``ls.circuit.circuitscape_pairwise``, circuitscape.py:550-670), solved on the GPU.
+
+    ``habitat``: resistances (or conductances), NaN / -9999 = NoData.  ``points``: a raster of focal ids (0 / NoData
+    elsewhere) or :class:`FocalPoints`.  ``polygons``: short-circuit region ids; ``mask``: cells where it is not
+    positive are removed; ``included_pairs``: :class:`IncludedPairs` or a path.  The map options keep each pair's
+    voltage / current map in ``result.maps`` (keys ``("voltage", id1, id2)`` / ``("current", id1, id2)``) and the
+    sum / maximum of the current maps.  ``n_threads`` is accepted for compatibility; ``tol`` is the CG's relative
+    residual target.
+    """
+    del n_threads
+    cells = _grid(habitat, "habitat")
+    g = habitat_conductance(cells, is_resistance=habitat_is_resistance, reclass=reclass)
+    poly = None
+    if polygons is not None:
+        pm = _grid(polygons, "polygons")
+        if pm.shape != g.shape:
+            raise ValueError("the polygons must have the habitat's shape")
+        pm[pm == NODATA] = 0
+        if not np.all(pm == np.round(pm)):
+            raise ValueError("the polygon raster must hold integer ids")
+        poly = pm.astype(np.int64)
+    if mask is not None:
+        m = _grid(mask, "mask")
+        if m.shape != g.shape:
+            raise ValueError("the mask must have the habitat's shape")
+        m[m == NODATA] = 0
+        g = g * np.where(m > 0, 1.0, 0.0)
+        if g.sum() == 0:
+            raise ValueError("Mask file deleted everything!")
+    if not isinstance(points, FocalPoints):
+        pm = _grid(points, "points")
+        if pm.shape != g.shape:
+            raise ValueError("the points must have the habitat's shape")
+        points = _points_from_map(pm)
+    if included_pairs is not None and not isinstance(included_pairs, IncludedPairs):
+        included_pairs = read_included_pairs(included_pairs)
+    points, excluded = _apply_included_pairs(points, included_pairs)
+    o = PairOptions(volt_maps=voltage_maps, cur_maps=current_maps, cum=current_maps or cum_map, max=max_map, focal_zero=set_focal_node_currents_to_zero,
+                    null_currents=set_null_currents_to_nodata, null_voltages=set_null_voltages_to_nodata,
+                    log_transform=log_transform_maps)
+    maps: dict = {}
+    ids = points.ids
+
+    def emit(ci, cj, volt, cur):
+        key = (int(ids[ci]), int(ids[cj]))
+        if volt is not None:
+            maps[("voltage", *key)] = volt
+        if cur is not None:
+            maps[("current", *key)] = cur
+
+    res, cum, mx, stats = _run_pairwise(g, poly, points, excluded, four_neighbors, avg_resistances, o, emit, tol,
+                                        device)
+    return CircuitscapeResult(resistances=res, cum_current=cum, max_current=mx, maps=maps, stats=stats)
+
+
+# --- INI files (circuitscape.py:977-1213, pairwise scenario) ---------------------------------------------------------
+
+DEFAULTS = {
+    "data_type": "raster", "scenario": "not entered", "connect_four_neighbors_only": "False",
+    "connect_using_avg_resistances": "False", "use_polygons": "False", "use_mask": "False", "mask_file": "None",
+    "habitat_file": "(Browse for a resistance file)", "habitat_map_is_resistances": "True",
+    "use_included_pairs": "False", "included_pairs_file": "(Browse for a file with pairs to include or exclude)",
+    "point_file": "(Browse for file with locations of focal points or regions)", "use_reclass_table": "False",
+    "reclass_file": "(Browse for file with reclassification data)", "write_cur_maps": "False",
+    "write_volt_maps": "False", "write_cum_cur_map_only": "False", "write_max_cur_maps": "False",
+    "set_null_currents_to_nodata": "False", "set_null_voltages_to_nodata": "False",
+    "set_focal_node_currents_to_zero": "False", "log_transform_maps": "False",
+    "polygon_file": "(Browse for a short-circuit region file)",
+}
+
+
+def parse_config(path) -> dict:
+    """Every line but ``[section]`` ones split at its first ``=`` (key right-stripped, value stripped)."""
+    cfg = {}
+    with open(path, encoding="utf-8") as f:
+        for line in f:
+            if line.startswith("["):
+                continue
+            key, sep, value = line.partition("=")
+            if sep:
+                cfg[key.rstrip()] = value.strip()
+    return cfg
+
+
+def _unset(path: str) -> bool:
+    return path == "" or path == "None" or path.startswith("(")
+
+
+def _flag(cfg, key) -> bool:
+    v = cfg[key]
+    if v in TRUELIST:
+        return True
+    if v in FALSELIST:
+        return False
+    raise ValueError(f'{key} = "{v}": expected True or False')
+
+
+def _resolve(name: str, base: Path) -> Path:
+    p = Path(name)
+    if p.is_absolute() or p.exists():
+        return p
+    q = base / p
+    return q if q.exists() else p
+
+
+def circuitscape_ini(path, *, write_outputs: bool = False, tol: float = 1e-13, device=None) -> CircuitscapeResult:
+    """Run a Circuitscape INI file of the pairwise scenario on rasters; paths are read from the working directory,
+    or else next to the INI file.  ``maps`` are keyed ``voltmap_<id1>_<id2>`` / ``curmap_<id1>_<id2>``.  Writing
+    output files is not supported (``write_outputs`` must be False)."""
+    if write_outputs:
+        raise NotImplementedError("writing Circuitscape output files is not supported")
+    path = Path(path)
+    base = path.resolve().parent
+    cfg = {**DEFAULTS, **parse_config(path)}
+    if cfg["data_type"] not in ("raster", "Raster"):
+        raise NotImplementedError(f'data_type = "{cfg["data_type"]}": only rasters are supported')
+    if cfg["scenario"] not in ("pairwise", "Pairwise"):
+        raise NotImplementedError(f'scenario = "{cfg["scenario"]}": only the pairwise scenario is supported')
+    for key in ("low_memory_mode", "preemptive_memory_release"):
+        if cfg.get(key, "False") in TRUELIST:
+            raise ValueError(f"{key} is not implemented in Circuitscape.jl; remove it or set it to False")
+
+    def need(key):
+        if _unset(cfg[key]):
+            raise ValueError(f"{key} is not set")
+        p = _resolve(cfg[key], base)
+        if not p.is_file():
+            raise FileNotFoundError(f'{key} = "{cfg[key]}" does not exist')
+        return p
+
+    cells, meta = read_raster(need("habitat_file"))
+    reclass = read_reclass_table(need("reclass_file")) if _flag(cfg, "use_reclass_table") else None
+    g = habitat_conductance(cells, is_resistance=_flag(cfg, "habitat_map_is_resistances"), reclass=reclass)
+    poly = None
+    if _flag(cfg, "use_polygons"):
+        poly = read_polymap(need("polygon_file"), meta, integer=True).astype(np.int64)
+    if _flag(cfg, "use_mask"):
+        m = read_polymap(need("mask_file"), meta)
+        g = g * np.where(m > 0, 1.0, 0.0)
+        if g.sum() == 0:
+            raise ValueError("Mask file deleted everything!")
+    points = read_point_map(need("point_file"), meta)
+    pairs = read_included_pairs(need("included_pairs_file")) if _flag(cfg, "use_included_pairs") else None
+    points, excluded = _apply_included_pairs(points, pairs)
+    cur, cum_only = _flag(cfg, "write_cur_maps"), _flag(cfg, "write_cum_cur_map_only")
+    o = PairOptions(volt_maps=_flag(cfg, "write_volt_maps"), cur_maps=cur and not cum_only, cum=cur or cum_only,
+                    max=_flag(cfg, "write_max_cur_maps"), focal_zero=_flag(cfg, "set_focal_node_currents_to_zero"),
+                    null_currents=_flag(cfg, "set_null_currents_to_nodata"),
+                    null_voltages=_flag(cfg, "set_null_voltages_to_nodata"),
+                    log_transform=_flag(cfg, "log_transform_maps"))
+    maps: dict = {}
+    ids = points.ids
+
+    def emit(ci, cj, volt, curmap):
+        name = f"_{int(ids[ci])}_{int(ids[cj])}"
+        if volt is not None:
+            maps["voltmap" + name] = volt
+        if curmap is not None:
+            maps["curmap" + name] = curmap
+
+    res, cum, mx, stats = _run_pairwise(g, poly, points, excluded, _flag(cfg, "connect_four_neighbors_only"),
+                                        _flag(cfg, "connect_using_avg_resistances"), o, emit, tol, device)
+    return CircuitscapeResult(resistances=res, cum_current=cum, max_current=mx, maps=maps, stats=stats)

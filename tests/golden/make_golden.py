@@ -9,10 +9,14 @@ landschaft source tree).  Reads the reference's own test data:
   Circuitscape advanced-mode solves (CHOLMOD node currents);
 * ``tests/data/reference/circuit/omniscape_ini/*.ini``, ``omniscape_input/*``
   (ASCII grids and a reclass table) and ``omniscape_ini.npz``: 11 Omniscape.jl
-  INI runs (the CHOLMOD outputs; the cg+amg outputs are left out).
+  INI runs (the CHOLMOD outputs; the cg+amg outputs are left out);
+* ``tests/data/reference/circuit/circuitscape/input/raster/pairwise/*`` and the
+  ``sgVerify*`` entries of ``circuitscape.npz``: Circuitscape's 17 pairwise INI
+  cases (resistance matrices and current / voltage maps).
 
-Writes ``omniscape_golden.npz``, ``advanced_golden.npz``, ``omniscape_ini.npz``
-and copies of the INI and input files (same layout) next to this file.
+Writes ``omniscape_golden.npz``, ``advanced_golden.npz``, ``omniscape_ini.npz``,
+``circuitscape/pairwise.npz`` and copies of the INI and input files (same
+layout) next to this file.
 The GPU machines do not have the reference tree, so the tests read only these
 fixtures.
 """
@@ -50,6 +54,16 @@ def main():
         (HERE / sub).mkdir(exist_ok=True)
         for f in sorted((data / sub).iterdir()):
             (HERE / sub / f.name).write_bytes(f.read_bytes())
+    cs = data / "circuitscape"
+    z = np.load(data / "circuitscape.npz")
+    out_dir = HERE / "circuitscape"
+    out_dir.mkdir(exist_ok=True)
+    np.savez_compressed(out_dir / "pairwise.npz", **{k: z[k] for k in z.files if k.startswith("sgVerify")})
+    for f in sorted((cs / "input" / "raster" / "pairwise").rglob("*")):
+        if f.is_file():
+            dst = out_dir / f.relative_to(cs)
+            dst.parent.mkdir(parents=True, exist_ok=True)
+            dst.write_bytes(f.read_bytes())
 
 
 if __name__ == "__main__":

@@ -39,7 +39,8 @@ def test_struct_layouts_match_the_header(tmp_path):
     if not shutil.which("gcc"):
         pytest.skip("no C compiler")
     fields = {"lsb_omni_condition": N.Condition, "lsb_omni_params": N.Params, "lsb_omni_stats": N.Stats,
-              "lsb_raster_params": N.RasterParams}
+              "lsb_raster_params": N.RasterParams, "lsb_graph_params": N.GraphParams,
+              "lsb_graph_stats": N.GraphStats}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "lsb_omniscape.h"', "int main(void) {"]
     for cname, py in fields.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')

@@ -1,0 +1,147 @@
+"""Circuitscape pairwise mode, host side: the oracle against Circuitscape's goldens, the package's node graph
+against the oracle's, the readers, and the C ABI's argument checks (no GPU)."""
+
+from __future__ import annotations
+
+import ctypes as C
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from landschaft_b200 import _native as N
+from landschaft_b200 import circuitscape as cs
+
+ROOT = Path(__file__).resolve().parents[1]
+CS = ROOT / "tests" / "golden" / "circuitscape"
+sys.path.insert(0, str(ROOT / "oracle"))
+import circuitscape_oracle as O  # noqa: E402
+
+POINT_CASES = ["sgVerify2", "sgVerify4", "sgVerify7", "sgVerify12", "sgVerify13", "sgVerify14", "sgVerify15",
+               "sgVerify16", "sgVerify17"]
+REGION_CASES = ["sgVerify3", "sgVerify5", "sgVerify6", "sgVerify8", "sgVerify9", "sgVerify10", "sgVerify11"]
+
+
+def ini_path(name):
+    return f"input/raster/pairwise/{name.removeprefix('sgVerify')}/{name}.ini"
+
+
+@pytest.fixture
+def in_cs(monkeypatch):
+    # the INI files hold paths relative to Circuitscape's test directory
+    monkeypatch.chdir(CS)
+
+
+def check_against_golden(name, res, cum, mx, maps):
+    z = np.load(CS / "pairwise.npz")
+    ref = z[f"{name}/result.txt"]
+    np.testing.assert_allclose(res, ref, rtol=1e-8, atol=1e-12)
+    for key, ours in (("cum_curmap.asc", cum), ("max_curmap.asc", mx)):
+        if f"{name}/{key}" in z.files:
+            want = z[f"{name}/{key}"]
+            np.testing.assert_allclose(ours, want, rtol=1e-9, atol=1e-11 * np.abs(want).max())
+    theirs = {k.split("/")[1][:-4] for k in z.files if k.startswith(name + "/")
+              and k.split("/")[1].startswith(("curmap_", "voltmap_"))}
+    assert set(maps) == theirs
+    for kind in theirs:
+        want = z[f"{name}/{kind}.asc"]
+        np.testing.assert_allclose(maps[kind], want, rtol=1e-9, atol=1e-11 * max(np.abs(want).max(), 1e-300))
+
+
+@pytest.mark.parametrize("name", POINT_CASES)
+def test_oracle_matches_circuitscape(name, in_cs):
+    check_against_golden(name, *O.pairwise_ini(ini_path(name)))
+
+
+def random_case(rng, ny, nx, polygons):
+    g = np.exp(rng.normal(size=(ny, nx)))
+    g[rng.random((ny, nx)) < 0.2] = 0
+    poly = None
+    if polygons:
+        poly = np.zeros((ny, nx), dtype=np.int64)
+        for pid in range(1, 4):
+            y, x = rng.integers(0, ny), rng.integers(0, nx)
+            poly[y:y + rng.integers(1, 4), x:x + rng.integers(1, 4)] = pid
+    return g, poly
+
+
+@pytest.mark.parametrize("avg", [False, True])
+@pytest.mark.parametrize("four", [False, True])
+def test_node_graph_matches_the_oracle(avg, four):
+    rng = np.random.default_rng(1 + 2 * avg + four)
+    for trial in range(25):
+        ny, nx = (int(v) for v in rng.integers(1, 14, 2))
+        g, poly = random_case(rng, ny, nx, trial % 2 == 1)
+        a = cs.raster_graph(g, poly, avg, four)
+        b = O.raster_graph(g, poly, avg, four)
+        assert a.n_nodes == b["n_nodes"] and a.n_comp == b["n_comp"]
+        np.testing.assert_array_equal(a.nodemap, b["nodemap"])
+        np.testing.assert_array_equal(a.comp, b["comp"])
+        np.testing.assert_array_equal(a.adj, np.array([r for row in b["rows"] for r, _ in row], dtype=np.int32))
+        np.testing.assert_array_equal(a.w, np.array([w for row in b["rows"] for _, w in row]))
+        np.testing.assert_array_equal(a.degree, b["degree"])
+
+
+def test_merged_nodes_and_zero_weight_edges():
+    # a non-habitat cell inside a polygon joins its node; with average resistances its edges weigh 0 and do not
+    # connect components
+    g = np.array([[1.0, 0.0, 1.0], [0.0, 0.0, 0.0], [1.0, 0.0, 1.0]])
+    poly = np.array([[1, 1, 0], [0, 0, 0], [0, 0, 0]])
+    a = cs.raster_graph(g, poly, True, True)
+    assert a.n_nodes == 4 and a.nodemap[0] == a.nodemap[1]
+    b = cs.raster_graph(g, poly, False, True)
+    assert a.n_comp == 4 and b.n_comp == 3  # average conductance joins (0,2) through the merged cell
+
+
+def test_readers(in_cs):
+    assert cs.file_type("input/raster/pairwise/2/cellmap.asc") == "aagrid"
+    assert cs.file_type("input/raster/pairwise/13/include_matrix.txt") == "pairs_aagrid"
+    assert cs.file_type("input/raster/pairwise/17/pairs_to_include.txt") == "pairs"
+    assert cs.file_type("input/raster/pairwise/7/points5x5.txt") == "list"
+    assert cs.file_type("input/raster/pairwise/1/polygons.tif") == "geotiff"
+    cells, meta = cs.read_raster("input/raster/pairwise/15/cellmap.asc.gz")
+    assert cells.shape == (meta.nrows, meta.ncols) == (10, 10)
+    p = cs.read_included_pairs("input/raster/pairwise/17/pairs_to_include.txt")
+    assert p.mode == "include" and 1 in p.ids
+    with pytest.raises(NotImplementedError):
+        cs.read_raster("input/raster/pairwise/1/polygons.tif")
+
+
+@pytest.mark.parametrize("name", REGION_CASES[:2])
+def test_focal_regions_are_rejected_before_any_solve(name, in_cs):
+    with pytest.raises(NotImplementedError):
+        cs.circuitscape_ini(ini_path(name))
+
+
+def test_ini_errors(tmp_path):
+    ini = tmp_path / "a.ini"
+    ini.write_text("[Options]\nscenario = one-to-all\n")
+    with pytest.raises(NotImplementedError):
+        cs.circuitscape_ini(ini)
+    ini.write_text("[Options]\nscenario = pairwise\nuse_polygons = maybe\nhabitat_file = x.asc\n")
+    with pytest.raises(FileNotFoundError):
+        cs.circuitscape_ini(ini)
+
+
+def test_graph_abi_argument_checks():
+    lib = N.load()
+    p = N.default_graph_params()
+    assert (p.tol, p.accept, p.max_iter, p.max_ctas) == (1e-14, 1e-9, 0, 0)
+    nb = C.c_size_t(0)
+    assert lib.lsb_graph_pairs_workspace_size(0, 1, C.byref(p), C.byref(nb)) == N.LSB_ERR_ARGUMENT
+    assert lib.lsb_graph_pairs_workspace_size(10, -1, C.byref(p), C.byref(nb)) == N.LSB_ERR_ARGUMENT
+    assert lib.lsb_graph_pairs_workspace_size(1000, 7, C.byref(p), C.byref(nb)) == N.LSB_OK
+    assert nb.value >= 7 * 3 * 1000 * 8
+    err = C.create_string_buffer(256)
+    st = N.GraphStats()
+    # ground out of range, and an empty job list (returns before touching any device memory)
+    rc = lib.lsb_graph_pairs(5, None, None, None, None, 5, 1, None, None, C.byref(p), None, None, None, 0,
+                             C.byref(st), err, len(err), None)
+    assert rc == N.LSB_ERR_ARGUMENT and b"ground" in err.value
+    rc = lib.lsb_graph_pairs(5, None, None, None, None, 0, 0, None, None, C.byref(p), None, None, None, 0,
+                             C.byref(st), err, len(err), None)
+    assert rc == N.LSB_OK and st.jobs == 0
+    rc = lib.lsb_graph_pairs(5, None, None, None, None, 0, 2, None, None, C.byref(p), None, None, None, 0,
+                             C.byref(st), err, len(err), None)
+    assert rc == N.LSB_ERR_ARGUMENT

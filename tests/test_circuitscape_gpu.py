@@ -1,0 +1,177 @@
+"""Circuitscape pairwise mode on the GPU (lsb_graph_pairs) against Circuitscape's goldens and the oracle."""
+
+from __future__ import annotations
+
+import ctypes as C
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from landschaft_b200 import _native as N
+from landschaft_b200 import circuitscape as cs
+
+ROOT = Path(__file__).resolve().parents[1]
+sys.path.insert(0, str(ROOT / "tests"))
+sys.path.insert(0, str(ROOT / "oracle"))
+import circuitscape_oracle as O  # noqa: E402
+from test_circuitscape_cpu import CS, POINT_CASES, check_against_golden, ini_path, random_case  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture
+def in_cs(monkeypatch):
+    monkeypatch.chdir(CS)
+
+
+@pytest.mark.parametrize("name", POINT_CASES)
+def test_pairwise_matches_circuitscape(name, in_cs):
+    r = cs.circuitscape_ini(ini_path(name))
+    check_against_golden(name, r.resistances, r.cum_current, r.max_current, r.maps)
+    assert r.stats.failures == 0 and r.stats.jobs > 0
+
+
+def test_docstring_example():
+    resistance = np.ones((10, 10))
+    resistance[:, 5] = 10
+    points = np.zeros((10, 10), dtype=int)
+    points[1, 1], points[8, 1], points[5, 8] = 1, 2, 3
+    r = cs.circuitscape_pairwise(resistance, points, cum_map=True)
+    np.testing.assert_array_equal(r.resistances.round(4), [[0.0, 1.0, 2.0, 3.0], [1.0, 0.0, 0.8515, 0.8567],
+                                                          [2.0, 0.8515, 0.0, 0.8409], [3.0, 0.8567, 0.8409, 0.0]])
+    assert r.cum_current.shape == (10, 10)
+
+
+def oracle_pairwise(g, poly, pm, avg, four, opts, excluded_ids=frozenset()):
+    G = O.raster_graph(g, poly, avg, four)
+    fp = cs._points_from_map(pm)
+    rows, cols = fp.cells
+    nodes = np.array([G["nodemap"][r * g.shape[1] + c] for r, c in zip(rows, cols)], dtype=np.int64)
+    n = len(fp.ids)
+    ex = np.array([[(int(fp.ids[a]), int(fp.ids[b])) in excluded_ids for b in range(n)] for a in range(n)],
+                  dtype=bool)
+    maps = {}
+
+    def emit(ci, cj, vmap, cmap):
+        key = (int(fp.ids[ci]), int(fp.ids[cj]))
+        if vmap is not None:
+            maps[("voltage", *key)] = vmap.reshape(g.shape)
+        if cmap is not None:
+            maps[("current", *key)] = cmap.reshape(g.shape)
+
+    R, cum, mx = O.pairwise(G, g, nodes, ex, opts, emit)
+    return R, cum, mx, maps
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_random_rasters_match_the_oracle(seed):
+    rng = np.random.default_rng(100 + seed)
+    ny, nx = (int(v) for v in rng.integers(8, 40, 2))
+    g, poly = random_case(rng, ny, nx, seed % 2 == 0)
+    pm = np.zeros((ny, nx))
+    cells = rng.choice(ny * nx, size=6, replace=False)
+    pm.flat[cells] = rng.permutation(np.arange(1, 7))
+    avg, four = bool(seed & 1), bool(seed & 2)
+    flags = dict(voltage_maps=True, current_maps=True, max_map=True,
+                 set_focal_node_currents_to_zero=seed == 3, set_null_currents_to_nodata=seed == 4,
+                 set_null_voltages_to_nodata=seed == 4, log_transform_maps=seed == 5)
+    r = cs.circuitscape_pairwise(g, pm, habitat_is_resistance=False, polygons=poly, four_neighbors=four,
+                                 avg_resistances=avg, **flags)
+    opts = {"volt_maps": True, "cur_maps": True, "cum": True, "max": True, "focal_zero": seed == 3,
+            "null_currents": seed == 4, "null_voltages": seed == 4, "log_transform": seed == 5}
+    R, cum, mx, maps = oracle_pairwise(g, poly, pm, avg, four, opts)
+    np.testing.assert_allclose(r.resistances[1:, 1:], R, rtol=1e-9, atol=1e-12)
+    scale = max(np.abs(cum).max(), 1e-300)
+    np.testing.assert_allclose(r.cum_current, cum.reshape(ny, nx), rtol=1e-8, atol=1e-10 * scale)
+    np.testing.assert_allclose(r.max_current, mx.reshape(ny, nx), rtol=1e-8, atol=1e-10 * scale)
+    assert set(r.maps) == set(maps)
+    for k, want in maps.items():
+        np.testing.assert_allclose(r.maps[k], want, rtol=1e-8, atol=1e-10 * max(np.abs(want).max(), 1e-300),
+                                   err_msg=str(k))
+
+
+def test_shortcut_matches_full_solves_and_excluded_pairs():
+    rng = np.random.default_rng(7)
+    g, poly = random_case(rng, 30, 26, True)
+    pm = np.zeros((30, 26))
+    pm.flat[rng.choice(30 * 26, size=7, replace=False)] = np.arange(1, 8)
+    short = cs.circuitscape_pairwise(g, pm, habitat_is_resistance=False, polygons=poly)
+    full = cs.circuitscape_pairwise(g, pm, habitat_is_resistance=False, polygons=poly, cum_map=True)
+    np.testing.assert_allclose(full.resistances, short.resistances, rtol=1e-9, atol=1e-12)
+    R, _, _, _ = oracle_pairwise(g, poly, pm, False, False, {})
+    np.testing.assert_allclose(short.resistances[1:, 1:], R, rtol=1e-9, atol=1e-12)
+    pairs = cs.IncludedPairs("exclude", np.array([1, 2, 3]), np.array([[0, 1, 0], [1, 0, 0], [0, 0, 0]]))
+    ex = cs.circuitscape_pairwise(g, pm, habitat_is_resistance=False, polygons=poly, included_pairs=pairs)
+    R, _, _, _ = oracle_pairwise(g, poly, pm, False, False, {}, pairs.excluded())
+    np.testing.assert_allclose(ex.resistances[1:, 1:], R, rtol=1e-9, atol=1e-12)
+    assert ex.resistances[1, 2] == -1 and ex.resistances[2, 1] == -1
+
+
+def test_larger_raster_matches_the_oracle():
+    rng = np.random.default_rng(11)
+    ny, nx = 96, 80
+    g = 10 ** rng.uniform(0, 2, size=(ny, nx))
+    g[rng.random((ny, nx)) < 0.1] = 0
+    pm = np.zeros((ny, nx))
+    pm.flat[rng.choice(ny * nx, size=5, replace=False)] = np.arange(1, 6)
+    r = cs.circuitscape_pairwise(g, pm, habitat_is_resistance=False, cum_map=True, max_map=True)
+    R, cum, mx, _ = oracle_pairwise(g, None, pm, False, False, {"cum": True, "max": True})
+    np.testing.assert_allclose(r.resistances[1:, 1:], R, rtol=1e-9)
+    np.testing.assert_allclose(r.cum_current, cum.reshape(ny, nx), rtol=1e-8, atol=1e-10 * np.abs(cum).max())
+    np.testing.assert_allclose(r.max_current, mx.reshape(ny, nx), rtol=1e-8, atol=1e-10 * np.abs(cum).max())
+
+
+def solve_path(w, ground, src, dst, params):
+    """lsb_graph_pairs on a path graph 0 - 1 - ... - n-1 with conductances w; returns (rc, volt, cur, stats)."""
+    import torch
+    lib = N.load()
+    n = len(w) + 1
+    adj, wt, ptr = [], [], [0]
+    for i in range(n):
+        for k in (i - 1, i + 1):
+            if 0 <= k < n:
+                adj.append(k)
+                wt.append(w[min(i, k)])
+        ptr.append(len(adj))
+    diag = np.array([sum(wt[ptr[i]:ptr[i + 1]]) for i in range(n)]) + cs.K_SHIFT
+    dev = torch.device("cuda", 0)
+    t = lambda a, dt: torch.tensor(np.asarray(a), dtype=dt, device=dev)  # noqa: E731
+    d_ptr, d_adj, d_w, d_diag = t(ptr, torch.int64), t(adj, torch.int32), t(wt, torch.float64), t(diag, torch.float64)
+    d_src, d_dst = t(src, torch.int32), t(dst, torch.int32)
+    nj = len(src)
+    volt = torch.empty((nj, n), dtype=torch.float64, device=dev)
+    cur = torch.empty_like(volt)
+    nb = C.c_size_t(0)
+    assert lib.lsb_graph_pairs_workspace_size(n, nj, C.byref(params), C.byref(nb)) == 0
+    ws = torch.empty(nb.value, dtype=torch.uint8, device=dev)
+    st = N.GraphStats()
+    err = C.create_string_buffer(256)
+    rc = lib.lsb_graph_pairs(n, d_ptr.data_ptr(), d_adj.data_ptr(), d_w.data_ptr(), d_diag.data_ptr(), ground, nj,
+                             d_src.data_ptr(), d_dst.data_ptr(), C.byref(params), volt.data_ptr(), cur.data_ptr(),
+                             ws.data_ptr(), nb.value, C.byref(st), err, len(err),
+                             torch.cuda.current_stream().cuda_stream)
+    return rc, volt.cpu().numpy(), cur.cpu().numpy(), st, err.value
+
+
+def test_series_resistors_closed_form():
+    w = [2.0, 0.5, 4.0, 1.0]
+    rc, volt, cur, st, _ = solve_path(w, 4, [0, 1, 4], [4, 3, 0], N.default_graph_params())
+    assert rc == 0 and st.failures == 0 and st.jobs == 3
+    np.testing.assert_allclose(volt[0, 4] - volt[0, 0], sum(1 / x for x in w), rtol=1e-12)
+    np.testing.assert_allclose(volt[1, 3] - volt[1, 1], 1 / 0.5 + 1 / 4.0, rtol=1e-12)
+    np.testing.assert_allclose(volt[2, 0] - volt[2, 4], sum(1 / x for x in w), rtol=1e-12)
+    assert volt[0, 0] == 0.0  # relative to the source
+    np.testing.assert_allclose(cur[0], np.ones(5), rtol=1e-12)  # a unit current through every node
+    np.testing.assert_allclose(cur[1], [0, 1, 1, 1, 0], atol=1e-12)
+
+
+def test_iteration_cap_reports_failure():
+    p = N.default_graph_params()
+    p.max_iter = 1
+    rc, _, _, st, err = solve_path([1.0] * 30, 30, [0], [15], p)
+    assert rc == N.LSB_ERR_NOT_CONVERGED and st.failures == 1 and b"failed" in err
+    p = N.default_graph_params()
+    rc, _, _, st, _ = solve_path([1.0] * 30, 30, [0, 40], [15, 3], p)  # a node index out of range fails that job
+    assert rc == N.LSB_ERR_NOT_CONVERGED and st.failures == 1
