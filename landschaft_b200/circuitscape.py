@@ -8,9 +8,10 @@ through ``lsb_graph_pairs`` of the C ABI: one CTA per pair solves the component'
 Jacobi-preconditioned CG and computes the pair's node currents; the reference factorises each component once
 (CHOLMOD-like multifrontal Cholesky) and back-substitutes every pair.
 
-Scope: single-cell focal points (raster or text list), short-circuit polygons, masks, include/exclude pair files,
-reclass tables, and every pairwise map option.  Focal regions (several cells sharing an id, the reference's
-``raster_pairwise_regions``), GeoTIFF inputs and the other scenarios raise ``NotImplementedError``.
+Scope: focal points and focal regions (several cells sharing an id: a graph per pair, the reference's
+``raster_pairwise_regions``), raster or text-list point files, short-circuit polygons, masks, include/exclude pair
+files, reclass tables, and every pairwise map option.  GeoTIFF inputs and the other scenarios (advanced with
+polygons, one-to-all, all-to-one, networks) raise ``NotImplementedError``.
 """
 
 from __future__ import annotations
@@ -638,9 +639,80 @@ def _apply_included_pairs(points: FocalPoints, pairs: IncludedPairs | None):
     return points, pairs.excluded()
 
 
+def region_polymap(polymap, n: int, cells: np.ndarray, ids: np.ndarray, pt1: int, pt2: int) -> np.ndarray:
+    """The short-circuit regions of one pair of focal regions (circuitscape.cpp:749-779): without polygons the two
+    regions' cells; with polygons, each region of several cells becomes one new region together with every polygon
+    it overlaps."""
+    if polymap is None:
+        poly = np.zeros(n, dtype=np.int64)
+        poly[cells[ids == pt1]] = pt1
+        poly[cells[ids == pt2]] = pt2
+        return poly
+    poly = np.ascontiguousarray(polymap, dtype=np.int64).ravel().copy()
+    k = int(poly.max())
+    for pt in (pt1, pt2):
+        idx = cells[ids == pt]
+        if len(idx) == 1:
+            continue
+        k += 1
+        vals = np.unique(poly[idx][poly[idx] != 0])
+        if len(vals):
+            poly[np.isin(poly, vals)] = k
+        poly[idx] = k
+    return poly
+
+
+def _run_regions(g, poly, points: FocalPoints, excluded_ids: set, four, avg, o: PairOptions, emit, tol, device):
+    """pairwise_regions (circuitscape.cpp:781-866): every pair of distinct ids gets its own graph, its two regions
+    made short-circuit regions, and one solve between the nodes of their first cells."""
+    rows, cols = points.cells
+    cells = (rows * g.shape[1] + cols).astype(np.int64)
+    ids = points.ids
+    pts = np.unique(ids)
+    n = len(pts)
+    ex = np.zeros((n, n), dtype=bool)
+    if excluded_ids:
+        for a in range(n):
+            for b in range(n):
+                ex[a, b] = (int(pts[a]), int(pts[b])) in excluded_ids
+    R = np.full((n, n), -1.0)
+    ncell = g.size
+    cum = np.zeros(g.shape) if o.cum else None
+    mx = np.full(g.shape, NODATA) if o.max else None
+    stats = GraphSolveStats()
+    shape = poly.shape if poly is not None else g.shape
+    for i in range(n):
+        for j in range(i + 1, n):
+            if ex[i, j] or ex[j, i]:
+                continue
+            pm = region_polymap(poly, ncell, cells, ids, int(pts[i]), int(pts[j])).reshape(shape)
+            graph = raster_graph(g, pm, avg, four)
+            nodes = np.array([graph.nodemap[cells[np.flatnonzero(ids == pts[e])[0]]] for e in (i, j)])
+            got = []
+            r2, c2, m2 = raster_pairwise(graph, g, nodes, np.zeros((2, 2), dtype=bool), o,
+                                         lambda ci, cj, v, c: got.append((ci, cj, v, c)), tol=tol, device=device,
+                                         stats=stats)
+            R[i, j] = R[j, i] = r2[0, 1]
+            if cum is not None:
+                cum += c2
+            if mx is not None:
+                np.maximum(mx, m2, out=mx)
+            for ci, cj, v, c in got:
+                if emit is not None:
+                    emit(i if ci == 0 else j, i if cj == 0 else j, v, c)
+    np.fill_diagonal(R, 0.0)
+    if cum is not None:
+        cum = np.maximum(cum, NODATA)
+    res = np.zeros((n + 1, n + 1))
+    res[0, 1:] = pts
+    res[1:, 0] = pts
+    res[1:, 1:] = R
+    return res, cum, mx, stats
+
+
 def _run_pairwise(g, poly, points: FocalPoints, excluded_ids: set, four, avg, o: PairOptions, emit, tol, device):
     if points.has_regions:
-        raise NotImplementedError("focal regions (several cells per focal id) are not supported")
+        return _run_regions(g, poly, points, excluded_ids, four, avg, o, emit, tol, device)
     graph = raster_graph(g, poly, avg, four)
     rows, cols = points.cells
     cells = rows * g.shape[1] + cols
@@ -711,7 +783,7 @@ def circuitscape_pairwise(habitat, points, *, habitat_is_resistance: bool = True
                     null_currents=set_null_currents_to_nodata, null_voltages=set_null_voltages_to_nodata,
                     log_transform=log_transform_maps)
     maps: dict = {}
-    ids = points.ids
+    ids = np.unique(points.ids) if points.has_regions else points.ids
 
     def emit(ci, cj, volt, cur):
         key = (int(ids[ci]), int(ids[cj]))
@@ -821,7 +893,7 @@ def circuitscape_ini(path, *, write_outputs: bool = False, tol: float = 1e-13, d
                     null_voltages=_flag(cfg, "set_null_voltages_to_nodata"),
                     log_transform=_flag(cfg, "log_transform_maps"))
     maps: dict = {}
-    ids = points.ids
+    ids = np.unique(points.ids) if points.has_regions else points.ids
 
     def emit(ci, cj, volt, curmap):
         name = f"_{int(ids[ci])}_{int(ids[cj])}"

@@ -9,6 +9,7 @@ Laplacian directly (scipy's sparse LU) where the reference uses its own multifro
 - ``node_currents``: ``graph_node_currents``, ``circuitscape.cpp:38-77``;
 - ``pairwise``: ``raster_pairwise``, ``circuitscape.cpp:474-743`` (jobs, grounding at the component's last node,
   per-pair maps, the shortcut of ``update_voltmatrix!`` / ``update_shortcut_resistances!``);
+- ``region_polymap`` / ``pairwise_regions``: ``circuitscape.cpp:749-866`` (a graph per pair of focal regions);
 - ``pairwise_ini``: the pairwise branch of ``circuitscape_ini``, ``src/landschaft/circuit/circuitscape.py:1039-1170``.
 
 The file parsers (ASCII grids, point lists, pair files) are the package's own; the reference's golden outputs of
@@ -309,6 +310,67 @@ def pairwise(G, gmap, points, excluded, opts, emit=None):
     return R, cum, mx
 
 
+def region_polymap(polymap, n, cells, ids, pt1, pt2):
+    if polymap is None:
+        poly = [0] * n
+        for x in range(len(ids)):
+            if ids[x] == pt1:
+                poly[cells[x]] = pt1
+        for x in range(len(ids)):
+            if ids[x] == pt2:
+                poly[cells[x]] = pt2
+        return np.array(poly, dtype=np.int64)
+    poly = [int(v) for v in polymap.ravel()]
+    k = max(poly)
+    for pt in (pt1, pt2):
+        idx = [cells[x] for x in range(len(ids)) if ids[x] == pt]
+        if len(idx) == 1:
+            continue
+        k += 1
+        vals = sorted(set(poly[c] for c in idx if poly[c] != 0))
+        if vals:
+            poly = [k if v in vals else v for v in poly]
+        for c in idx:
+            poly[c] = k
+    return np.array(poly, dtype=np.int64)
+
+
+def pairwise_regions(gmap, polymap, avg, four, cells, ids, excluded, opts, emit=None):
+    """raster_pairwise_regions: ids sorted; `excluded` over the distinct ids."""
+    pts = sorted(set(int(v) for v in ids))
+    npt = len(pts)
+    ny, nx = gmap.shape
+    ncell = nx * ny
+    R = np.full((npt, npt), -1.0)
+    cum = np.zeros(ncell) if opts.get("cum") else None
+    mx = np.full(ncell, NODATA) if opts.get("max") else None
+    for i in range(npt):
+        for j in range(i + 1, npt):
+            if excluded[i, j] or excluded[j, i]:
+                continue
+            poly = region_polymap(polymap, ncell, cells, ids, pts[i], pts[j]).reshape(gmap.shape)
+            G = raster_graph(gmap, poly, avg, four)
+            nodes = []
+            for pt in (pts[i], pts[j]):
+                x = next(x for x in range(len(ids)) if ids[x] == pt)
+                nodes.append(int(G["nodemap"][cells[x]]))
+            got = []
+            r2, c2, m2 = pairwise(G, gmap, np.array(nodes), np.zeros((2, 2), dtype=bool), opts,
+                                  lambda ci, cj, v, c: got.append((ci, cj, v, c)))
+            R[i, j] = R[j, i] = r2[0, 1]
+            if cum is not None:
+                cum += c2
+            if mx is not None:
+                mx = np.maximum(mx, m2)
+            for ci, cj, v, c in got:
+                if emit is not None:
+                    emit(i if ci == 0 else j, i if cj == 0 else j, v, c)
+    np.fill_diagonal(R, 0.0)
+    if cum is not None:
+        cum = np.maximum(cum, NODATA)
+    return np.array(pts), R, cum, mx
+
+
 def pairwise_ini(path):
     """The pairwise scenario of an INI file: (resistance matrix with ids, cum map, max map, maps by name)."""
     from landschaft_b200 import circuitscape as cs
@@ -328,22 +390,41 @@ def pairwise_ini(path):
     points = cs.read_point_map(need("point_file"), meta)
     pairs = cs.read_included_pairs(need("included_pairs_file")) if cs._flag(cfg, "use_included_pairs") else None
     points, excluded_ids = cs._apply_included_pairs(points, pairs)
-    if points.has_regions:
-        raise NotImplementedError("focal regions")
     cur, cum_only = cs._flag(cfg, "write_cur_maps"), cs._flag(cfg, "write_cum_cur_map_only")
     opts = {"volt_maps": cs._flag(cfg, "write_volt_maps"), "cur_maps": cur and not cum_only, "cum": cur or cum_only,
             "max": cs._flag(cfg, "write_max_cur_maps"), "focal_zero": cs._flag(cfg, "set_focal_node_currents_to_zero"),
             "null_currents": cs._flag(cfg, "set_null_currents_to_nodata"),
             "null_voltages": cs._flag(cfg, "set_null_voltages_to_nodata"),
             "log_transform": cs._flag(cfg, "log_transform_maps")}
-    G = raster_graph(g, poly, cs._flag(cfg, "connect_using_avg_resistances"),
-                     cs._flag(cfg, "connect_four_neighbors_only"))
+    avg, four = cs._flag(cfg, "connect_using_avg_resistances"), cs._flag(cfg, "connect_four_neighbors_only")
     rows, cols = points.cells
+    maps = {}
+    if points.has_regions:
+        cells = [int(r * g.shape[1] + c) for r, c in zip(rows, cols)]
+        pts = sorted(set(int(v) for v in points.ids))
+        n = len(pts)
+        ex = np.array([[(pts[a], pts[b]) in excluded_ids for b in range(n)] for a in range(n)], dtype=bool)
+
+        def emit_r(ci, cj, vmap, cmap):
+            name = f"_{pts[ci]}_{pts[cj]}"
+            if vmap is not None:
+                maps["voltmap" + name] = vmap.reshape(g.shape)
+            if cmap is not None:
+                maps["curmap" + name] = cmap.reshape(g.shape)
+
+        ids_r, R, cum, mx = pairwise_regions(g, poly, avg, four, cells, [int(v) for v in points.ids], ex, opts,
+                                             emit_r)
+        res = np.zeros((n + 1, n + 1))
+        res[0, 1:] = ids_r
+        res[1:, 0] = ids_r
+        res[1:, 1:] = R
+        return (res, None if cum is None else cum.reshape(g.shape), None if mx is None else mx.reshape(g.shape),
+                maps)
+    G = raster_graph(g, poly, avg, four)
     nodes = np.array([G["nodemap"][r * g.shape[1] + c] for r, c in zip(rows, cols)], dtype=np.int64)
     ids = points.ids
     n = len(ids)
     ex = np.array([[(int(ids[a]), int(ids[b])) in excluded_ids for b in range(n)] for a in range(n)], dtype=bool)
-    maps = {}
 
     def emit(ci, cj, vmap, cmap):
         name = f"_{int(ids[ci])}_{int(ids[cj])}"

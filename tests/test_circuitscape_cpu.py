@@ -49,7 +49,7 @@ def check_against_golden(name, res, cum, mx, maps):
         np.testing.assert_allclose(maps[kind], want, rtol=1e-9, atol=1e-11 * max(np.abs(want).max(), 1e-300))
 
 
-@pytest.mark.parametrize("name", POINT_CASES)
+@pytest.mark.parametrize("name", POINT_CASES + REGION_CASES)
 def test_oracle_matches_circuitscape(name, in_cs):
     check_against_golden(name, *O.pairwise_ini(ini_path(name)))
 
@@ -108,10 +108,21 @@ def test_readers(in_cs):
         cs.read_raster("input/raster/pairwise/1/polygons.tif")
 
 
-@pytest.mark.parametrize("name", REGION_CASES[:2])
-def test_focal_regions_are_rejected_before_any_solve(name, in_cs):
-    with pytest.raises(NotImplementedError):
-        cs.circuitscape_ini(ini_path(name))
+def test_region_polymap_matches_the_oracle():
+    rng = np.random.default_rng(5)
+    for trial in range(30):
+        ny, nx = (int(v) for v in rng.integers(3, 12, 2))
+        poly = None
+        if trial % 2:
+            poly = np.zeros((ny, nx), dtype=np.int64)
+            for pid in range(1, 4):
+                y, x = rng.integers(0, ny), rng.integers(0, nx)
+                poly[y:y + 3, x:x + 2] = pid
+        cells = rng.choice(ny * nx, size=7, replace=False).astype(np.int64)
+        ids = np.sort(rng.integers(1, 4, size=7))
+        for a, b in ((1, 2), (1, 3), (2, 3)):
+            np.testing.assert_array_equal(cs.region_polymap(poly, ny * nx, cells, ids, a, b),
+                                          O.region_polymap(poly, ny * nx, list(cells), list(ids), a, b))
 
 
 def test_ini_errors(tmp_path):

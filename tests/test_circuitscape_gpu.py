@@ -16,7 +16,8 @@ ROOT = Path(__file__).resolve().parents[1]
 sys.path.insert(0, str(ROOT / "tests"))
 sys.path.insert(0, str(ROOT / "oracle"))
 import circuitscape_oracle as O  # noqa: E402
-from test_circuitscape_cpu import CS, POINT_CASES, check_against_golden, ini_path, random_case  # noqa: E402
+from test_circuitscape_cpu import (CS, POINT_CASES, REGION_CASES, check_against_golden, ini_path,  # noqa: E402
+                                   random_case)
 
 pytestmark = pytest.mark.gpu
 
@@ -26,7 +27,7 @@ def in_cs(monkeypatch):
     monkeypatch.chdir(CS)
 
 
-@pytest.mark.parametrize("name", POINT_CASES)
+@pytest.mark.parametrize("name", POINT_CASES + REGION_CASES)
 def test_pairwise_matches_circuitscape(name, in_cs):
     r = cs.circuitscape_ini(ini_path(name))
     check_against_golden(name, r.resistances, r.cum_current, r.max_current, r.maps)
@@ -121,6 +122,39 @@ def test_larger_raster_matches_the_oracle():
     np.testing.assert_allclose(r.resistances[1:, 1:], R, rtol=1e-9)
     np.testing.assert_allclose(r.cum_current, cum.reshape(ny, nx), rtol=1e-8, atol=1e-10 * np.abs(cum).max())
     np.testing.assert_allclose(r.max_current, mx.reshape(ny, nx), rtol=1e-8, atol=1e-10 * np.abs(cum).max())
+
+
+@pytest.mark.parametrize("polygons", [False, True])
+def test_focal_regions_match_the_oracle(polygons):
+    rng = np.random.default_rng(21 + polygons)
+    ny, nx = 18, 15
+    g, poly = random_case(rng, ny, nx, polygons)
+    pm = np.zeros((ny, nx))
+    pm.flat[rng.choice(ny * nx, size=9, replace=False)] = np.repeat([1, 2, 3, 4], [3, 2, 3, 1])
+    r = cs.circuitscape_pairwise(g, pm, habitat_is_resistance=False, polygons=poly, current_maps=True,
+                                 voltage_maps=True, max_map=True)
+    fp = cs._points_from_map(pm)
+    rows, cols = fp.cells
+    cells = [int(a * nx + b) for a, b in zip(rows, cols)]
+    maps = {}
+
+    def emit(ci, cj, vmap, cmap):
+        key = (ci + 1, cj + 1)
+        if vmap is not None:
+            maps[("voltage", *key)] = vmap.reshape(ny, nx)
+        if cmap is not None:
+            maps[("current", *key)] = cmap.reshape(ny, nx)
+
+    opts = {"volt_maps": True, "cur_maps": True, "cum": True, "max": True}
+    ids, R, cum, mx = O.pairwise_regions(g, poly, False, False, cells, [int(v) for v in fp.ids],
+                                         np.zeros((4, 4), dtype=bool), opts, emit)
+    np.testing.assert_array_equal(r.resistances[0, 1:], ids)
+    np.testing.assert_allclose(r.resistances[1:, 1:], R, rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(r.cum_current, cum.reshape(ny, nx), rtol=1e-8, atol=1e-10 * np.abs(cum).max())
+    np.testing.assert_allclose(r.max_current, mx.reshape(ny, nx), rtol=1e-8, atol=1e-10 * np.abs(cum).max())
+    assert set(r.maps) == set(maps)
+    for k, want in maps.items():
+        np.testing.assert_allclose(r.maps[k], want, rtol=1e-8, atol=1e-10 * max(np.abs(want).max(), 1e-300))
 
 
 def solve_path(w, ground, src, dst, params):
