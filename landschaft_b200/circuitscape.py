@@ -81,8 +81,10 @@ def read_raster(path):
     p = os.fspath(path)
     if not os.path.isfile(p):
         raise FileNotFoundError(f'the file "{p}" does not exist')
+    if file_type(p) == "geotiff":
+        return _read_tiff(p)
     if not p.lower().removesuffix(".gz").endswith(".asc"):
-        raise NotImplementedError(f"{p}: only ESRI ASCII grids are read (no GeoTIFF reader in this package)")
+        raise NotImplementedError(f"{p}: only ESRI ASCII grids and uncompressed GeoTIFFs are read")
     header: dict[str, float] = {}
     rows = []
     with _open(p) as f:
@@ -105,6 +107,51 @@ def read_raster(path):
     nodata = header.get("nodata_value", NODATA)
     a[(a == nodata) | np.isnan(a)] = NODATA
     return a, RasterMeta(nrows, ncols, xll, yll, dx)
+
+
+_TIFF_SIZES = {1: 1, 2: 1, 3: 2, 4: 4, 5: 8, 6: 1, 7: 1, 8: 2, 9: 4, 10: 8, 11: 4, 12: 8, 16: 8}
+
+
+def _read_tiff(path):
+    """A single-band, uncompressed, strip-organised GeoTIFF (the baseline layout GDAL writes by default): values as
+    double with GDAL's nodata value (tag 42113) and NaN set to -9999; the grid from the pixel-scale and tiepoint
+    tags.  Other layouts raise NotImplementedError."""
+    import struct
+    with (gzip.open if os.fspath(path).lower().endswith("gz") else open)(path, "rb") as f:
+        b = f.read()
+    end = {b"II": "<", b"MM": ">"}.get(b[:2])
+    if end is None or struct.unpack_from(end + "H", b, 2)[0] != 42:
+        raise NotImplementedError(f"{path}: not a classic TIFF")
+    off = struct.unpack_from(end + "I", b, 4)[0]
+    tags = {}
+    for k in range(struct.unpack_from(end + "H", b, off)[0]):
+        tag, typ, cnt, _ = struct.unpack_from(end + "HHII", b, off + 2 + 12 * k)
+        size = _TIFF_SIZES.get(typ, 1) * cnt
+        pos = off + 2 + 12 * k + 8 if size <= 4 else struct.unpack_from(end + "I", b, off + 2 + 12 * k + 8)[0]
+        raw = b[pos:pos + size]
+        fmt = {3: "H", 4: "I", 8: "h", 9: "i", 11: "f", 12: "d", 16: "Q"}.get(typ)
+        tags[tag] = raw.rstrip(b"\0").decode() if typ == 2 else (struct.unpack(f"{end}{cnt}{fmt}", raw) if fmt
+                                                                else raw)
+    ncols, nrows = tags[256][0], tags[257][0]
+    bits = tags.get(258, (1,))[0]
+    fmt_code = tags.get(339, (1,))[0]
+    if tags.get(259, (1,))[0] != 1 or tags.get(277, (1,))[0] != 1 or 322 in tags or 273 not in tags:
+        raise NotImplementedError(f"{path}: only single-band, uncompressed, strip-organised TIFFs are read")
+    kind = {1: "u", 2: "i", 3: "f"}[fmt_code]
+    dtype = np.dtype(f"{end}{kind}{bits // 8}")
+    data = b"".join(b[o:o + c] for o, c in zip(tags[273], tags[279]))
+    a = np.frombuffer(data, dtype=dtype, count=nrows * ncols).reshape(nrows, ncols).astype(np.float64)
+    if 42113 in tags and tags[42113]:
+        nodata = float(tags[42113])
+        if kind != "f":
+            nodata = float(np.array(nodata).astype(np.int64))
+        a[a == nodata] = NODATA
+    a[np.isnan(a)] = NODATA
+    sx, sy = (tags[33550][0], tags[33550][1]) if 33550 in tags else (1.0, 1.0)
+    ti, tj, _, tx, ty, _ = tags[33922] if 33922 in tags else (0.0, 0.0, 0.0, 0.0, float(nrows), 0.0)
+    xll = tx - ti * sx
+    yll = ty + tj * sy - nrows * sy
+    return a, RasterMeta(nrows, ncols, xll, yll, sx)
 
 
 def _read_rows(path) -> list:

@@ -18,7 +18,7 @@ CS = ROOT / "tests" / "golden" / "circuitscape"
 sys.path.insert(0, str(ROOT / "oracle"))
 import circuitscape_oracle as O  # noqa: E402
 
-POINT_CASES = ["sgVerify2", "sgVerify4", "sgVerify7", "sgVerify12", "sgVerify13", "sgVerify14", "sgVerify15",
+POINT_CASES = ["sgVerify1", "sgVerify2", "sgVerify4", "sgVerify7", "sgVerify12", "sgVerify13", "sgVerify14", "sgVerify15",
                "sgVerify16", "sgVerify17"]
 REGION_CASES = ["sgVerify3", "sgVerify5", "sgVerify6", "sgVerify8", "sgVerify9", "sgVerify10", "sgVerify11"]
 
@@ -104,8 +104,13 @@ def test_readers(in_cs):
     assert cells.shape == (meta.nrows, meta.ncols) == (10, 10)
     p = cs.read_included_pairs("input/raster/pairwise/17/pairs_to_include.txt")
     assert p.mode == "include" and 1 in p.ids
-    with pytest.raises(NotImplementedError):
-        cs.read_raster("input/raster/pairwise/1/polygons.tif")
+    tif, meta = cs.read_raster("input/raster/pairwise/1/polygons.tif")
+    asc, _ = cs.read_raster("input/raster/pairwise/1/polygons.asc")
+    assert (meta.nrows, meta.ncols) == (10, 10)
+    np.testing.assert_array_equal(tif, asc)
+    tif, meta = cs.read_raster("input/raster/pairwise/10/cellmap7.tif")
+    asc, meta2 = cs.read_raster("input/raster/pairwise/11/cellmap7.asc")
+    assert (meta.nrows, meta.ncols) == (meta2.nrows, meta2.ncols)
 
 
 def test_region_polymap_matches_the_oracle():
