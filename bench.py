@@ -247,6 +247,100 @@ def kernel_time(lsb_om, rt, st, params, flush, reps=3):
 ADV_METRIC = "advanced-mode rasters/s: 4096 independent grounded raster circuits, FP32 CG + FP64 refinement"
 
 
+PW_METRIC = "Circuitscape pairwise: pair solves/s (unit current between two focal nodes, node currents included)"
+
+
+def bench_pairwise(args, rank, world, local, d):
+    """Circuitscape's pairwise mode with current maps on a 256 x 256 raster with 24 focal points (276 pairs, every
+    pair solved); a step is one lsb_graph_pairs call over all pairs of the component (device-resident system)."""
+    import torch
+    from landschaft_b200 import circuitscape as cs, synthetic
+    r, pm = synthetic.pairwise_256(rank)
+    dev = torch.device("cuda", local)
+    g = cs.habitat_conductance(np.where(np.isnan(r), cs.NODATA, r))
+    graph = cs.raster_graph(g, None, False, False)
+    fp = cs._points_from_map(pm)
+    rows, cols = fp.cells
+    nodes = graph.nodemap[rows * g.shape[1] + cols]
+    k = graph.comp[nodes[0]]
+    nodes = nodes[graph.comp[nodes] == k]
+    members = np.flatnonzero(graph.comp == k)
+    sys_ = cs.component_system(graph, members)
+    dsys = cs.system_to_device(sys_, dev)
+    ground = int(sys_.local[members[-1]])
+    pairs = [(a, b) for a in range(len(nodes)) for b in range(a + 1, len(nodes))]
+    src = torch.tensor([int(sys_.local[nodes[a]]) for a, _ in pairs], dtype=torch.int32, device=dev)
+    dst = torch.tensor([int(sys_.local[nodes[b]]) for _, b in pairs], dtype=torch.int32, device=dev)
+    n, nj = len(members), len(pairs)
+    _, _, st = cs.solve_pairs(dsys, ground, src, dst)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for _ in range(args.warmup):
+        cs.solve_pairs(dsys, ground, src, dst, stats=False)
+    clocks = Clocks(local)
+    d.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    times = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        cs.solve_pairs(dsys, ground, src, dst, stats=False)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+    clk = clocks.stop()
+    d.barrier()
+    T = d.max(sum(times))
+    # end to end: the public call from host rasters (graph, solves, maps)
+    te = []
+    for _ in range(max(1, min(args.steps, 2))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = cs.circuitscape_pairwise(r, pm, cum_map=True, device=dev)
+        te.append(time.perf_counter() - t0)
+    TE = d.max(sum(te) / len(te))
+    err = None
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, str(Path(__file__).resolve().parent / "oracle"))
+        import circuitscape_oracle as O
+        G = O.raster_graph(g, None, False, False)
+        mem = [v for v in range(G["n_nodes"]) if G["comp"][v] == k]
+        t0 = time.perf_counter()
+        loc, lu = O._component_solver(G, mem, mem[-1])
+        R = np.zeros(len(pairs))
+        for q, (a, b) in enumerate(pairs):
+            bvec = np.zeros(len(loc))
+            s_, d_ = int(nodes[a]), int(nodes[b])
+            if s_ in loc:
+                bvec[loc[s_]] = -1.0
+            if d_ in loc:
+                bvec[loc[d_]] = 1.0
+            x = lu.solve(bvec)
+            R[q] = (x[loc[d_]] if d_ in loc else 0.0) - (x[loc[s_]] if s_ in loc else 0.0)
+        dt = time.perf_counter() - t0
+        ours = np.array([res.resistances[1 + a, 1 + b] for a, b in pairs])
+        err = float(np.max(np.abs(ours - R) / np.abs(R)))
+        cpu = {"value": nj / dt, "unit": "pairs/s", "cores": 1, "kind": "port",
+               "sample": f"the oracle: the component's sparse LU (scipy SuperLU, one thread) and all {nj} pair solves "
+                         "(resistances only, no currents); the reference factorises once the same way"}
+    if rank == 0:
+        line = {"metric": PW_METRIC, "value": world * nj * args.steps / T, "unit": "pairs/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * T / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded Gaussian random field, 24 random focal points)",
+                "config": {"workload": "pairwise_256", "nodes": n, "pairs": nj, "neighbours": 8,
+                           "l2": "flushed between timed steps (256 MiB write)", "tol": 1e-14},
+                "e2e": {"value": world * nj / TE, "unit": "pairs/s", "h2d_bytes_per_step": int(2 * 8 * g.size),
+                        "d2h_bytes_per_step": int(nj * 2 * 8 * n), "includes": "host graph build and map assembly"},
+                "cg_iterations": {"mean": st.iters_mean, "max": st.iters_max}, "ctas": st.ctas,
+                "worst_residual": st.worst_residual, "max_rel_err_vs_oracle": err, "clocks": clk,
+                "gpu_launches": args.steps, "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    d.close()
+
+
 def bench_advanced(args, rank, world, local, d):
     """The advanced-mode batch: 4096 rasters of sides U{64..512}, log-uniform resistance in [1, 1000], one unit
     source and one direct ground each, 4 neighbours; a step is one launch over the whole batch."""
@@ -385,6 +479,8 @@ def main():
 
     if args.workload == "advanced_4096":
         return bench_advanced(args, rank, world, local, d)
+    if args.workload == "pairwise_256":
+        return bench_pairwise(args, rank, world, local, d)
     r, s, kw = synthetic.WORKLOADS[args.workload](rank)
     if args.crop:
         y0, x0 = (r.shape[0] - args.crop) // 2, (r.shape[1] - args.crop) // 2

@@ -424,63 +424,101 @@ class GraphSolveStats:
     failures: int = 0
 
 
-def _solve_component(graph: RasterGraph, members: np.ndarray, ground: int, src: np.ndarray, dst: np.ndarray,
-                     want_currents: bool, params, stats: GraphSolveStats, device):
-    """Every job (src, dst node) on one component: unit current into dst, out of src, the ground node at 0 V.
-    Returns (volt, cur) as numpy arrays of jobs x members: the voltages relative to the source node, and the node
-    currents (None without ``want_currents``)."""
-    import torch
-    lib = N.load()
+@dataclass
+class ComponentSystem:
+    """One component's grounded Laplacian in the form lsb_graph_pairs takes: its nodes (ascending), the
+    graph-node -> local-index table, and the CSR rows (edges leaving the component dropped; they weigh 0) with the
+    diagonal plus the reference factorisation's shift."""
+
+    members: np.ndarray
+    local: np.ndarray
+    ptr: np.ndarray
+    adj: np.ndarray
+    w: np.ndarray
+    diag: np.ndarray
+
+
+def component_system(graph: RasterGraph, members: np.ndarray) -> ComponentSystem:
     m = len(members)
     local = np.full(graph.n_nodes, -1, dtype=np.int64)
     local[members] = np.arange(m)
     lens = graph.ptr[members + 1] - graph.ptr[members]
     idx = np.repeat(graph.ptr[members], lens) + (np.arange(lens.sum()) - np.repeat(np.cumsum(lens) - lens, lens))
     la = local[graph.adj[idx]]
-    keep = la >= 0  # edges leaving the component carry no conductance
+    keep = la >= 0
     rowid = np.repeat(np.arange(m), lens)[keep]
     ptr = np.zeros(m + 1, dtype=np.int64)
     np.add.at(ptr, rowid + 1, 1)
-    ptr = np.cumsum(ptr)
-    adj = la[keep].astype(np.int32)
-    w = graph.w[idx][keep]
-    diag = graph.degree[members] + K_SHIFT
-    dev = device
-    t = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).to(dev)  # noqa: E731
-    d_ptr, d_adj, d_w, d_diag = t(ptr, np.int64), t(adj, np.int32), t(w, np.float64), t(diag, np.float64)
-    js, jd = local[src].astype(np.int32), local[dst].astype(np.int32)
+    return ComponentSystem(members, local, np.cumsum(ptr), la[keep].astype(np.int32), graph.w[idx][keep],
+                           graph.degree[members] + K_SHIFT)
+
+
+def system_to_device(sys_: ComponentSystem, device):
+    """(n, ptr, adj, w, diag) as device tensors."""
+    import torch
+    t = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).to(device)  # noqa: E731
+    return (len(sys_.members), t(sys_.ptr, np.int64), t(sys_.adj, np.int32), t(sys_.w, np.float64),
+            t(sys_.diag, np.float64))
+
+
+def solve_pairs(dsys, ground: int, src, dst, *, currents: bool = True, params=None, stats: bool = True):
+    """One lsb_graph_pairs call on the current stream: ``dsys`` from system_to_device, ``ground`` / ``src`` /
+    ``dst`` local node indices (src, dst: int32 device tensors).  Returns (volt, cur, GraphStats): jobs x n device
+    tensors (cur None without ``currents``) and the statistics (None with ``stats=False``, which does not wait)."""
+    import torch
+    lib = N.load()
+    n, d_ptr, d_adj, d_w, d_diag = dsys
+    params = params if params is not None else graph_params()
+    nb = int(src.numel())
+    dev = d_ptr.device
+    volt = torch.empty((nb, n), dtype=torch.float64, device=dev)
+    cur = torch.empty((nb, n), dtype=torch.float64, device=dev) if currents else None
+    nbytes = C.c_size_t(0)
+    rc = lib.lsb_graph_pairs_workspace_size(n, nb, C.byref(params), C.byref(nbytes))
+    N.check(rc, C.create_string_buffer(b"invalid graph size or parameters"))
+    ws = torch.empty(max(int(nbytes.value), 16), dtype=torch.uint8, device=dev)
+    st = N.GraphStats() if stats else None
+    err = C.create_string_buffer(1024)
+    rc = lib.lsb_graph_pairs(n, d_ptr.data_ptr(), d_adj.data_ptr(), d_w.data_ptr(), d_diag.data_ptr(), int(ground),
+                             nb, src.data_ptr(), dst.data_ptr(), C.byref(params), volt.data_ptr(),
+                             cur.data_ptr() if cur is not None else None, ws.data_ptr(), ws.numel(),
+                             C.byref(st) if st is not None else None, err, len(err),
+                             torch.cuda.current_stream(dev).cuda_stream)
+    N.check(rc, err)
+    return volt, cur, st
+
+
+def _solve_component(graph: RasterGraph, members: np.ndarray, ground: int, src: np.ndarray, dst: np.ndarray,
+                     want_currents: bool, params, stats: GraphSolveStats, device):
+    """Every job (src, dst node) on one component: unit current into dst, out of src, the ground node at 0 V.
+    Returns (volt, cur) as numpy arrays of jobs x members: the voltages relative to the source node, and the node
+    currents (None without ``want_currents``)."""
+    import torch
+    sys_ = component_system(graph, members)
+    dsys = system_to_device(sys_, device)
+    m = len(members)
+    js, jd = sys_.local[src].astype(np.int32), sys_.local[dst].astype(np.int32)
     nj = len(js)
     volt = np.empty((nj, m))
     cur = np.empty((nj, m)) if want_currents else None
-    # jobs in batches of bounded output size
-    per = max(1, min(nj, (1 << 27) // max(m * 16, 1)))
+    per = max(1, min(nj, (1 << 27) // max(m * 16, 1)))  # jobs per call: outputs of at most 128 MiB
     for b0 in range(0, nj, per):
         b1 = min(nj, b0 + per)
         nb = b1 - b0
-        d_src, d_dst = t(js[b0:b1], np.int32), t(jd[b0:b1], np.int32)
-        d_v = torch.empty((nb, m), dtype=torch.float64, device=dev)
-        d_c = torch.empty((nb, m), dtype=torch.float64, device=dev) if want_currents else None
-        nbytes = C.c_size_t(0)
-        rc = lib.lsb_graph_pairs_workspace_size(m, nb, C.byref(params), C.byref(nbytes))
-        N.check(rc, C.create_string_buffer(b"invalid graph size or parameters"))
-        ws = torch.empty(max(int(nbytes.value), 16), dtype=torch.uint8, device=dev)
-        st = N.GraphStats()
-        err = C.create_string_buffer(1024)
-        stream = torch.cuda.current_stream(dev)
-        rc = lib.lsb_graph_pairs(m, d_ptr.data_ptr(), d_adj.data_ptr(), d_w.data_ptr(), d_diag.data_ptr(),
-                                 int(local[ground]), nb, d_src.data_ptr(), d_dst.data_ptr(), C.byref(params),
-                                 d_v.data_ptr(), d_c.data_ptr() if d_c is not None else None, ws.data_ptr(),
-                                 ws.numel(), C.byref(st), err, len(err), stream.cuda_stream)
-        N.check(rc, err)
-        volt[b0:b1] = d_v.cpu().numpy()
+        d_src = torch.from_numpy(js[b0:b1]).to(device)
+        d_dst = torch.from_numpy(jd[b0:b1]).to(device)
+        try:
+            v, c, st = solve_pairs(dsys, int(sys_.local[ground]), d_src, d_dst, currents=want_currents,
+                                   params=params)
+        except N.NativeError:
+            stats.failures += nb
+            raise
+        volt[b0:b1] = v.cpu().numpy()
         if want_currents:
-            cur[b0:b1] = d_c.cpu().numpy()
+            cur[b0:b1] = c.cpu().numpy()
         stats.iters_mean = (stats.iters_mean * stats.jobs + st.iters_mean * nb) / (stats.jobs + nb)
         stats.jobs += nb
         stats.iters_max = max(stats.iters_max, int(st.iters_max))
-        stats.failures += int(st.failures)
-    if stats.failures:
-        raise N.NativeError(f"{stats.failures} pair solves did not converge")
     return volt, cur
 
 

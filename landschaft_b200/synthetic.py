@@ -117,6 +117,18 @@ def omni_4096(seed: int = 0):
     return r, s, dict(radius=64, block_size=5, buffer=0, four_neighbors=False)
 
 
+def pairwise_256(seed: int = 0, n_points: int = 24):
+    """Circuitscape pairwise workload: a 256 x 256 resistance raster (the Omniscape workloads' Gaussian random field,
+    r = 10^(2g) in [1, 100], 1% NoData in 3 x 3 clusters) and `n_points` focal points with ids 1..n_points on
+    distinct random cells with data.  Returns (resistance with NaN NoData, point raster)."""
+    r, _ = omni_grf(256, seed)
+    rng = np.random.default_rng(seed + 7)
+    ok = np.flatnonzero(np.isfinite(r).ravel())
+    pm = np.zeros(r.shape)
+    pm.flat[rng.choice(ok, size=n_points, replace=False)] = np.arange(1, n_points + 1)
+    return r, pm
+
+
 def _advanced_draws(rng, side_min, side_max):
     ny, nx = (int(v) for v in rng.integers(side_min, side_max + 1, 2))
     r = np.exp(rng.uniform(np.log(1.0), np.log(1000.0), (ny, nx)))
