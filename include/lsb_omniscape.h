@@ -284,6 +284,24 @@ int lsb_graph_pairs(int64_t n, const int64_t *ptr, const int32_t *adj, const dou
                     const lsb_graph_params *p, double *volt, double *cur, void *workspace, size_t workspace_bytes,
                     lsb_graph_stats *stats, char *err, size_t errlen, void *stream);
 
+/* Advanced-mode problems on one component (Circuitscape's advanced mode on node graphs, and one-to-all /
+ * all-to-one, whose problems are one per focal point).  Replaces, per component and problem, the factorisation and
+ * solve of circuit::raster_advanced / raster_advanced_many (src/cpp/circuit/circuitscape.cpp:393-470,904-1083) and
+ * graph_node_currents with finite grounds (circuitscape.cpp:38-77).  The component is given as for
+ * lsb_graph_pairs, with diag WITHOUT finite grounds.  Job j lists, as CSR over the jobs: its current sources
+ * (src_node / src_val over src_ptr[j] .. src_ptr[j + 1]), its direct grounds held at 0 V (dir_node over dir_ptr) and
+ * its finite grounds, added to the diagonal (fin_node / fin_val over fin_ptr); nodes are unique within each list,
+ * and a direct ground's own source is ignored.  volt[j n + i] = the voltage of node i; cur[j n + i] (when
+ * cur != NULL) = max(inflow, outflow), the current through a finite ground included.  All pointers but stats and
+ * err are device pointers. */
+int lsb_graph_solve_workspace_size(int64_t n, int64_t n_jobs, const lsb_graph_params *p, size_t *bytes);
+int lsb_graph_solve(int64_t n, const int64_t *ptr, const int32_t *adj, const double *w, const double *diag,
+                    int64_t n_jobs, const int64_t *src_ptr, const int32_t *src_node, const double *src_val,
+                    const int64_t *dir_ptr, const int32_t *dir_node, const int64_t *fin_ptr,
+                    const int32_t *fin_node, const double *fin_val, const lsb_graph_params *p, double *volt,
+                    double *cur, void *workspace, size_t workspace_bytes, lsb_graph_stats *stats, char *err,
+                    size_t errlen, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -14,7 +14,8 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB = PKG / "liblsb_omni.so"
-SOURCES = ([CSRC / "omni_capi.cu", CSRC / "omni_adv.cu", CSRC / "omni_win_128_hot.cu", CSRC / "graph_pairs.cu"] +
+SOURCES = ([CSRC / "omni_capi.cu", CSRC / "omni_adv.cu", CSRC / "omni_win_128_hot.cu", CSRC / "graph_pairs.cu",
+            CSRC / "graph_solve.cu"] +
            [CSRC / f"omni_win_{nt}_{kind}.cu" for nt in (256, 512) for kind in ("hot", "gen")])
 DEPS = SOURCES + sorted(CSRC.glob("*.cuh")) + [PKG.parent / "include" / "lsb_omniscape.h"]
 

@@ -22,7 +22,8 @@ EXPORTS = ("lsb_params_default", "lsb_omniscape_workspace_size", "lsb_omniscape"
            "lsb_omniscape_grad", "lsb_omniscape_grad_workspace_size", "lsb_last_launch_count",
            "lsb_time_window_kernels", "lsb_version", "lsb_omniscape_noalloc", "lsb_tune_set", "lsb_tune_get",
            "lsb_tune_clear", "lsb_raster_params_default", "lsb_rasters_workspace_size", "lsb_rasters",
-           "lsb_graph_params_default", "lsb_graph_pairs_workspace_size", "lsb_graph_pairs")
+           "lsb_graph_params_default", "lsb_graph_pairs_workspace_size", "lsb_graph_pairs",
+           "lsb_graph_solve_workspace_size", "lsb_graph_solve")
 
 
 class Condition(C.Structure):
@@ -132,6 +133,12 @@ def load():
         lib.lsb_graph_pairs.argtypes = [i64, vp, vp, vp, vp, i32, i64, vp, vp, C.POINTER(GraphParams), vp, vp, vp,
                                         sz, C.POINTER(GraphStats), C.c_char_p, sz, vp]
         lib.lsb_graph_pairs.restype = C.c_int
+        lib.lsb_graph_solve_workspace_size.argtypes = [i64, i64, C.POINTER(GraphParams), C.POINTER(sz)]
+        lib.lsb_graph_solve_workspace_size.restype = C.c_int
+        lib.lsb_graph_solve.argtypes = [i64, vp, vp, vp, vp, i64, vp, vp, vp, vp, vp, vp, vp, vp,
+                                        C.POINTER(GraphParams), vp, vp, vp, sz, C.POINTER(GraphStats), C.c_char_p,
+                                        sz, vp]
+        lib.lsb_graph_solve.restype = C.c_int
         _lib = lib
         return lib
 

@@ -699,6 +699,9 @@ class CircuitscapeResult:
     max_current: np.ndarray | None = None
     maps: dict = field(default_factory=dict)
     stats: GraphSolveStats | None = None
+    voltage: np.ndarray | None = None   # advanced mode: per-cell maps (0 on cells without a node)
+    current: np.ndarray | None = None
+    nodemap: np.ndarray | None = None
 
 
 def _grid(value, name) -> np.ndarray:
@@ -882,7 +885,435 @@ def circuitscape_pairwise(habitat, points, *, habitat_is_resistance: bool = True
     return CircuitscapeResult(resistances=res, cum_current=cum, max_current=mx, maps=maps, stats=stats)
 
 
-# --- INI files (circuitscape.py:977-1213, pairwise scenario) ---------------------------------------------------------
+# --- advanced mode, one-to-all, all-to-one (circuitscape.cpp:382-470,870-1083; circuitscape.py:406-516,704-955) ----
+
+POLICIES = ("keepall", "rmvsrc", "rmvgnd", "rmvall")
+
+
+def node_sums(graph: RasterGraph, cells: np.ndarray, vals: np.ndarray) -> np.ndarray:
+    """Per-node sums of cell values, cells taken in column-major order (stable), zeros skipped."""
+    cells = np.asarray(cells, dtype=np.int64)
+    vals = np.asarray(vals, dtype=np.float64)
+    s = np.zeros(graph.n_nodes)
+    if len(cells) == 0:
+        return s
+    order = np.lexsort((cells // graph.nx, cells % graph.nx))
+    c, v = cells[order], vals[order]
+    node = graph.nodemap[c]
+    keep = (node >= 0) & (v != 0)
+    np.add.at(s, node[keep], v[keep])  # unbuffered: repeated nodes add in the order given
+    return s
+
+
+def resolve_conflicts(src: np.ndarray, gnd: np.ndarray, policy: str):
+    """Finite grounds (taken before the policy), then the policy on nodes with both a source and a ground, then no
+    direct ground under a positive source (circuitscape.cpp:881-900).  Returns (src, gnd, finite)."""
+    finite = np.where(gnd < np.inf, gnd, 0.0)
+    both = (src != 0) & (gnd != 0)
+    if policy in ("rmvsrc", "rmvall"):
+        src = np.where(both, 0.0, src)
+    elif policy == "rmvgnd":
+        gnd = np.where(both, 0.0, gnd)
+    gnd = np.where((gnd == np.inf) & (src > 0), 0.0, gnd)
+    return src, gnd, finite
+
+
+def solve_problems(dsys, jobs, *, currents: bool = True, params=None, stats: bool = True):
+    """One lsb_graph_solve call: ``jobs`` lists (src_nodes, src_vals, direct_nodes, finite_nodes, finite_vals) in
+    local node indices.  Returns (volt, cur, GraphStats) as in solve_pairs."""
+    import torch
+    lib = N.load()
+    n, d_ptr, d_adj, d_w, d_diag = dsys
+    params = params if params is not None else graph_params()
+    dev = d_ptr.device
+    nb = len(jobs)
+
+    def csr(k):
+        lens = [len(j[k]) for j in jobs]
+        ptr = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+        nodes = np.concatenate([np.asarray(j[k], dtype=np.int32) for j in jobs]) if sum(lens) else np.zeros(1, np.int32)
+        return ptr, nodes
+
+    s_ptr, s_node = csr(0)
+    s_val = np.concatenate([np.asarray(j[1], dtype=np.float64) for j in jobs] + [np.zeros(1)])
+    d_ptr2, d_node = csr(2)
+    f_ptr, f_node = csr(3)
+    f_val = np.concatenate([np.asarray(j[4], dtype=np.float64) for j in jobs] + [np.zeros(1)])
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    T = [t(a) for a in (s_ptr, s_node, s_val, d_ptr2, d_node, f_ptr, f_node, f_val)]
+    volt = torch.empty((nb, n), dtype=torch.float64, device=dev)
+    cur = torch.empty((nb, n), dtype=torch.float64, device=dev) if currents else None
+    nbytes = C.c_size_t(0)
+    rc = lib.lsb_graph_solve_workspace_size(n, nb, C.byref(params), C.byref(nbytes))
+    N.check(rc, C.create_string_buffer(b"invalid graph size or parameters"))
+    ws = torch.empty(max(int(nbytes.value), 16), dtype=torch.uint8, device=dev)
+    st = N.GraphStats() if stats else None
+    err = C.create_string_buffer(1024)
+    rc = lib.lsb_graph_solve(n, d_ptr.data_ptr(), d_adj.data_ptr(), d_w.data_ptr(), d_diag.data_ptr(), nb,
+                             *(x.data_ptr() for x in T), C.byref(params), volt.data_ptr(),
+                             cur.data_ptr() if cur is not None else None, ws.data_ptr(), ws.numel(),
+                             C.byref(st) if st is not None else None, err, len(err),
+                             torch.cuda.current_stream(dev).cuda_stream)
+    N.check(rc, err)
+    return volt, cur, st
+
+
+def advanced_many(graph: RasterGraph, srcs, gnds, only_nodes, policy: str, *, tol=1e-13, device=None,
+                  stats: GraphSolveStats | None = None):
+    """raster_advanced_many (circuitscape.cpp:904-1083) on the GPU: every problem (per-node sources and grounds,
+    +inf a direct ground) is solved in each component that holds a nonzero source sum and a nonzero ground sum
+    (only the component of its check node when only_nodes[p] >= 0; none when it is -2).  Returns per problem a dict
+    with the node voltages and currents, the active nodes and whether anything was solved."""
+    import torch
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    params = graph_params(tol)
+    stats = stats if stats is not None else GraphSolveStats()
+    n = graph.n_nodes
+    res = [resolve_conflicts(np.asarray(s, dtype=np.float64), np.asarray(g_, dtype=np.float64), policy)
+           for s, g_ in zip(srcs, gnds)]
+    out = [{"voltage": np.zeros(n), "current": np.zeros(n), "solved": False,
+            "active": np.flatnonzero((r[0] != 0) | (r[1] != 0)).astype(np.int32)} for r in res]
+    order = np.argsort(graph.comp, kind="stable")
+    bounds = np.searchsorted(graph.comp[order], np.arange(graph.n_comp + 1))
+    for k in range(graph.n_comp):
+        members = order[bounds[k]:bounds[k + 1]]
+        probs = []
+        for p, (s, g_, _) in enumerate(res):
+            only = int(only_nodes[p])
+            if only == -2 or (only >= 0 and graph.comp[only] != k):
+                continue
+            if np.cumsum(s[members])[-1] != 0 and np.cumsum(g_[members])[-1] != 0:
+                probs.append(p)
+                out[p]["solved"] = True
+        if not probs:
+            continue
+        sys_ = component_system(graph, members)
+        dsys = system_to_device(sys_, dev)
+        jobs = []
+        for p in probs:
+            s, g_, fin = res[p]
+            sm, gm, fm = s[members], g_[members], fin[members]
+            nz = np.flatnonzero(sm != 0)
+            fz = np.flatnonzero(fm != 0)
+            jobs.append((nz, sm[nz], np.flatnonzero(gm == np.inf), fz, fm[fz]))
+        v, c, st = solve_problems(dsys, jobs, params=params)
+        v, c = v.cpu().numpy(), c.cpu().numpy()
+        for q, p in enumerate(probs):
+            out[p]["voltage"][members] = v[q]
+            out[p]["current"][members] = c[q]
+        stats.iters_mean = (stats.iters_mean * stats.jobs + st.iters_mean * len(probs)) / (stats.jobs + len(probs))
+        stats.jobs += len(probs)
+        stats.iters_max = max(stats.iters_max, int(st.iters_max))
+    return out
+
+
+def multi_advanced(g, poly, avg: bool, four: bool, problems, policy: str, *, tol=1e-13, device=None, stats=None):
+    """The reference's native circuitscape_multi_advanced on the GPU: one graph, many problems given by cells
+    (src_cells / src_vals / gnd_cells / gnd_vals, check_cell -1 or a cell whose component alone is solved).
+    Returns (nodemap, results)."""
+    graph = raster_graph(g, poly, avg, four)
+    srcs, gnds, only = [], [], []
+    for q in problems:
+        srcs.append(node_sums(graph, q["src_cells"], q["src_vals"]))
+        gnds.append(node_sums(graph, q["gnd_cells"], q["gnd_vals"]))
+        o = -1
+        if q["check_cell"] >= 0:
+            o = int(graph.nodemap[q["check_cell"]])
+            if o < 0:
+                o = -2
+        only.append(o)
+    return graph.nodemap.reshape(g.shape), advanced_many(graph, srcs, gnds, only, policy, tol=tol, device=device,
+                                                         stats=stats)
+
+
+def _advanced(g, poly, src, gnd, four, avg, policy, unit, direct, solver) -> CircuitscapeResult:
+    """circuitscape.py:499-516: one problem over the whole raster."""
+    if unit:
+        src = np.where(src != 0, 1.0, src)
+    if direct:
+        gnd = np.where(gnd != 0, np.inf, gnd)
+    sc, gc = np.flatnonzero(src.ravel() != 0), np.flatnonzero(gnd.ravel() != 0)
+    prob = {"src_cells": sc, "src_vals": src.ravel()[sc], "gnd_cells": gc, "gnd_vals": gnd.ravel()[gc],
+            "check_cell": -1}
+    nm, (r,) = solver(g, poly, avg, four, [prob], policy)
+    on = nm >= 0
+    volt = np.zeros(nm.shape)
+    cur = np.zeros(nm.shape)
+    volt[on] = r["voltage"][nm[on]]
+    cur[on] = r["current"][nm[on]]
+    res = CircuitscapeResult(voltage=volt, current=cur, nodemap=nm)
+    res.maps["solved"] = bool(r["solved"])
+    return res
+
+
+def circuitscape_advanced(habitat, source, ground, *, habitat_is_resistance: bool = True,
+                          ground_is_resistance: bool = True, polygons=None, mask=None, four_neighbors: bool = False,
+                          avg_resistances: bool = False, remove_src_or_gnd: str = "keepall",
+                          unit_currents: bool = False, direct_grounds: bool = False, reclass: dict | None = None,
+                          n_threads: int = 0, tol: float = 1e-13, device=None) -> CircuitscapeResult:
+    """Circuitscape's advanced mode on a node graph (drop-in for ``ls.circuit.circuitscape_advanced``,
+    circuitscape.py:406-497): sources and grounds per cell (grounds as resistances unless ``ground_is_resistance``
+    is False; 0 / inf = direct), short-circuit polygons, a mask, the conflict policy, unit currents and direct
+    grounds.  Returns ``voltage`` and ``current`` maps (0 on cells without a node) and the ``nodemap``."""
+    del n_threads
+    if remove_src_or_gnd not in POLICIES:
+        raise ValueError(f"remove_src_or_gnd must be one of {POLICIES}")
+    g, poly = _habitat_and_polygons(habitat, habitat_is_resistance, reclass, polygons, mask)
+    src = _grid(source, "source")
+    gnd = _grid(ground, "ground")
+    if src.shape != g.shape or gnd.shape != g.shape:
+        raise ValueError("the source and ground must have the habitat's shape")
+    src[src == NODATA] = 0.0
+    nod = gnd == NODATA
+    if ground_is_resistance:
+        with np.errstate(divide="ignore"):
+            gnd = 1 / gnd
+    gnd[nod] = 0.0
+    solver = lambda *a: multi_advanced(*a, tol=tol, device=device)  # noqa: E731
+    return _advanced(g, poly, src, gnd, four_neighbors, avg_resistances, remove_src_or_gnd, unit_currents,
+                     direct_grounds, solver)
+
+
+def _point_polymap(polymap, point_map: np.ndarray, ids: np.ndarray) -> np.ndarray:
+    """create_new_polymap with a point map (circuitscape.py:712-735): focal points and regions become polygons."""
+    if polymap is None:
+        return point_map.astype(np.int64)
+    newpoly = polymap.copy()
+    no_regions = len(ids) == len(np.unique(ids))
+    jj, ii = np.nonzero(point_map.T)  # column-major
+    if no_regions:
+        k = polymap.max()
+        for r, c in zip(ii, jj):
+            if polymap[r, c] == 0:
+                newpoly[r, c] = point_map[r, c] + k
+        return newpoly
+    k = max(polymap.max(), point_map.max())
+    for r, c in zip(ii, jj):
+        v1, v2 = point_map[r, c], newpoly[r, c]
+        if v2 == 0:
+            newpoly[r, c] = k + v1
+            continue
+        if v1 != v2:
+            newpoly[newpoly == v2] = v1
+    return newpoly
+
+
+def read_point_strengths(path) -> np.ndarray:
+    """Two columns, id and strength (ids from 0 shifted to 1)."""
+    t = np.array(_read_rows(path), dtype=np.float64)
+    if t.ndim != 2 or t.shape[1] != 2:
+        raise ValueError(f"{path} must have exactly 2 columns")
+    if t[:, 0].min() == 0:
+        t[:, 0] += 1
+    return t
+
+
+def _one_to_all(g, poly, points: FocalPoints, strengths, pairs, one_to_all: bool, four, avg, opts: dict, emit,
+                solver) -> CircuitscapeResult:
+    """run_onetoall (circuitscape.py:737-851): one advanced-mode problem per focal id; one-to-all injects the id's
+    strength at its point with every other point a direct ground, all-to-one the reverse."""
+    ny, nx = g.shape
+    if pairs is not None:
+        keep = np.isin(points.ids, pairs.ids)
+        points = FocalPoints(points.rows[keep], points.cols[keep], points.ids[keep])
+        if strengths is not None:
+            strengths = strengths[np.isin(strengths[:, 0], pairs.ids)]
+    rows, cols = points.cells
+    cells = rows * nx + cols
+    ids = points.ids
+    point_map = np.zeros((ny, nx), dtype=np.int64)
+    point_map[rows, cols] = ids
+    unique_ids, first = np.unique(ids, return_index=True)
+    unique_map = np.zeros((ny, nx), dtype=np.int64)
+    unique_map[rows[first], cols[first]] = unique_ids
+    no_regions = len(ids) == len(unique_ids)
+    mode = 0 if pairs is not None and pairs.mode == "include" else 1
+    base_poly = _point_polymap(poly, point_map, ids)
+    res = np.zeros(len(unique_ids))
+    cum = np.zeros((ny, nx)) if opts["cum"] else None
+    mx = np.full((ny, nx), NODATA) if opts["max"] else None
+    policy = "rmvgnd" if one_to_all else "rmvsrc"
+
+    def problem(i):
+        n = int(unique_ids[i])
+        pm = point_map.copy()
+        newpoly = base_poly
+        strength = float(strengths[i, 1]) if strengths is not None else 1.0
+        if pairs is not None:
+            row = int(np.nonzero(pairs.ids == n)[0][0])
+            for j in range(len(pairs.ids)):
+                if j != row and pairs.matrix[row, j] == mode:
+                    pm[pm == pairs.ids[j]] = 0
+            if not no_regions:
+                newpoly = _point_polymap(poly, pm, ids)
+        smap = None
+        if strengths is not None:
+            st = strengths[:, 1].copy()
+            st[pm[rows, cols] == 0] = 1.0
+            smap = np.zeros((ny, nx))
+            smap[rows, cols] = st[: len(rows)]
+        if pm.sum() == n:
+            return None
+        if one_to_all:
+            src = np.where(unique_map == n, strength, 0.0)
+            gnd = np.where(pm == n, 0, pm).astype(np.float64)
+            gnd[gnd > 0] = np.inf
+        else:
+            if smap is not None:
+                src = np.where(unique_map == n, 0.0, smap)
+            else:
+                src = np.where(unique_map != 0, 1.0, 0.0)
+                src = np.where(pm == n, 0.0, src)
+            gnd = np.where(pm == n, np.inf, 0.0)
+        sc, gc = np.flatnonzero(src), np.flatnonzero(gnd)
+        return {"n": n, "strength": strength, "poly": newpoly, "src_cells": sc.astype(np.int64),
+                "src_vals": src.ravel()[sc], "gnd_cells": gc.astype(np.int64), "gnd_vals": gnd.ravel()[gc],
+                "check_cell": int(cells[np.nonzero(ids == n)[0][0]])}
+
+    probs = [(i, problem(i)) for i in range(len(unique_ids))]
+    for i, q in probs:
+        if q is None:
+            res[i] = -1
+    todo = [(i, q) for i, q in probs if q is not None]
+    # one solve call per graph (focal regions with included pairs rebuild it per point)
+    groups: list = []
+    for i, q in todo:
+        if groups and groups[-1][0] is q["poly"]:
+            groups[-1][1].append((i, q))
+        else:
+            groups.append((q["poly"], [(i, q)]))
+    solved = {}
+    for pm_, items in groups:
+        nm, results = solver(g, np.ascontiguousarray(pm_, dtype=np.int64), avg, four, [q for _, q in items], policy)
+        for (i, _), r in zip(items, results):
+            solved[i] = (nm, r)
+    for i, q in todo:
+        nm, r = solved[i]
+        n = q["n"]
+        if not r["solved"]:
+            res[i] = -1
+        elif not one_to_all:
+            res[i] = 0
+        else:
+            node = nm[unique_map == n][0]
+            val = 0.0 if node < 0 else r["voltage"][node] / q["strength"]
+            res[i] = -1 if val == 0 else val
+        on = nm >= 0
+        volt = np.zeros((ny, nx))
+        volt[on] = r["voltage"][nm[on]]
+        cur = np.zeros((ny, nx))
+        cur[on] = r["current"][nm[on]]
+        if opts["focal_zero"]:
+            cur[np.isin(nm, r["active"])] = 0.0
+        if cum is not None:
+            cum += cur
+        if mx is not None:
+            np.maximum(mx, cur, out=mx)
+        emit(n, volt if opts["volt_maps"] else None, cur if opts["cur_maps"] else None)
+    if cum is not None:
+        cum[cum < NODATA] = NODATA
+    if mx is not None:
+        mx[mx < NODATA] = NODATA
+    return CircuitscapeResult(resistances=np.column_stack([unique_ids.astype(np.float64), res]), cum_current=cum,
+                              max_current=mx)
+
+
+def _habitat_and_polygons(habitat, habitat_is_resistance, reclass, polygons, mask):
+    g = habitat_conductance(_grid(habitat, "habitat"), is_resistance=habitat_is_resistance, reclass=reclass)
+    poly = None
+    if polygons is not None:
+        pm = _grid(polygons, "polygons")
+        if pm.shape != g.shape:
+            raise ValueError("the polygons must have the habitat's shape")
+        pm[pm == NODATA] = 0
+        if not np.all(pm == np.round(pm)):
+            raise ValueError("the polygon raster must hold integer ids")
+        poly = pm.astype(np.int64)
+    if mask is not None:
+        m = _grid(mask, "mask")
+        if m.shape != g.shape:
+            raise ValueError("the mask must have the habitat's shape")
+        m[m == NODATA] = 0
+        g = g * np.where(m > 0, 1.0, 0.0)
+        if g.sum() == 0:
+            raise ValueError("Mask file deleted everything!")
+    return g, poly
+
+
+def circuitscape_one_to_all(habitat, points, *, all_to_one: bool = False, habitat_is_resistance: bool = True,
+                            polygons=None, mask=None, four_neighbors: bool = False, avg_resistances: bool = False,
+                            included_pairs=None, strengths=None, voltage_maps: bool = False,
+                            current_maps: bool = False, cum_map: bool = False, max_map: bool = False,
+                            set_focal_node_currents_to_zero: bool = False, reclass: dict | None = None,
+                            n_threads: int = 0, tol: float = 1e-13, device=None) -> CircuitscapeResult:
+    """Circuitscape's one-to-all (or, with ``all_to_one``, all-to-one) mode on rasters (drop-in for
+    ``ls.circuit.circuitscape_one_to_all``, circuitscape.py:854-953).  ``resistances`` has the ids in its first
+    column and each point's result in the second (one-to-all: the voltage at the point per unit strength, -1 when
+    nothing was solved); ``maps`` keys ``("voltage", id)`` / ``("current", id)``."""
+    del n_threads
+    g, poly = _habitat_and_polygons(habitat, habitat_is_resistance, reclass, polygons, mask)
+    if not isinstance(points, FocalPoints):
+        pm = _grid(points, "points")
+        if pm.shape != g.shape:
+            raise ValueError("the points must have the habitat's shape")
+        points = _points_from_map(pm)
+    if included_pairs is not None and not isinstance(included_pairs, IncludedPairs):
+        included_pairs = read_included_pairs(included_pairs)
+    if strengths is not None and isinstance(strengths, (str, os.PathLike)):
+        strengths = read_point_strengths(strengths)
+    maps: dict = {}
+
+    def emit(n, volt, cur):
+        if volt is not None:
+            maps[("voltage", n)] = volt
+        if cur is not None:
+            maps[("current", n)] = cur
+
+    opts = {"volt_maps": voltage_maps, "cur_maps": current_maps, "cum": current_maps or cum_map, "max": max_map,
+            "focal_zero": set_focal_node_currents_to_zero}
+    solver = lambda *a: multi_advanced(*a, tol=tol, device=device)  # noqa: E731
+    r = _one_to_all(g, poly, points, None if strengths is None else np.asarray(strengths, dtype=np.float64),
+                    included_pairs, not all_to_one, four_neighbors, avg_resistances, opts, emit, solver)
+    r.maps = maps
+    return r
+
+
+def _read_list3(path) -> np.ndarray:
+    return np.array(_read_rows(path), dtype=np.float64).reshape(-1, 3)
+
+
+def _source_and_ground(source_path, ground_path, meta: RasterMeta, ground_is_res: bool):
+    """read_source_and_ground_maps (circuitscape.py:1230-1258)."""
+    kind = file_type(ground_path)
+    if kind in ("aagrid", "geotiff"):
+        gnd = read_polymap(ground_path, meta, nodata_as=None)
+    elif kind == "list":
+        pts = _read_list3(ground_path)
+        gnd = np.full((meta.nrows, meta.ncols), NODATA)
+        i, j = _list_cells(pts, meta)
+        gnd[i - 1, j - 1] = pts[:, 0]
+    else:
+        raise ValueError("Cannot recognise file type.")
+    kind = file_type(source_path)
+    if kind in ("aagrid", "geotiff"):
+        src = read_polymap(source_path, meta)
+        src[src == NODATA] = 0.0
+    elif kind == "list":
+        pts = _read_list3(source_path)
+        src = np.zeros((meta.nrows, meta.ncols))
+        i, j = _list_cells(pts, meta)
+        src[i - 1, j - 1] = pts[:, 0]
+    else:
+        raise ValueError("Cannot recognize file type.")
+    nod = gnd == NODATA
+    if ground_is_res:
+        with np.errstate(divide="ignore"):
+            gnd = 1 / gnd
+    gnd[nod] = 0.0
+    return src, gnd
+
+
+# --- INI files (circuitscape.py:977-1213) -------------------------------------------------------------------------
 
 DEFAULTS = {
     "data_type": "raster", "scenario": "not entered", "connect_four_neighbors_only": "False",
@@ -895,7 +1326,13 @@ DEFAULTS = {
     "set_null_currents_to_nodata": "False", "set_null_voltages_to_nodata": "False",
     "set_focal_node_currents_to_zero": "False", "log_transform_maps": "False",
     "polygon_file": "(Browse for a short-circuit region file)",
+    "source_file": "(Browse for a current source file)", "ground_file": "(Browse for a ground point file)",
+    "ground_file_is_resistances": "True", "use_unit_currents": "False", "use_direct_grounds": "False",
+    "remove_src_or_gnd": "keepall", "use_variable_source_strengths": "False", "variable_source_file": "None",
 }
+SCENARIOS = {"pairwise": "pairwise", "Pairwise": "pairwise", "advanced": "advanced", "Advanced": "advanced",
+             "one-to-all": "one-to-all", "one_to_all": "one-to-all", "all-to-one": "all-to-one",
+             "all_to_one": "all-to-one"}
 
 
 def parse_config(path) -> dict:
@@ -932,10 +1369,14 @@ def _resolve(name: str, base: Path) -> Path:
     return q if q.exists() else p
 
 
-def circuitscape_ini(path, *, write_outputs: bool = False, tol: float = 1e-13, device=None) -> CircuitscapeResult:
-    """Run a Circuitscape INI file of the pairwise scenario on rasters; paths are read from the working directory,
-    or else next to the INI file.  ``maps`` are keyed ``voltmap_<id1>_<id2>`` / ``curmap_<id1>_<id2>``.  Writing
-    output files is not supported (``write_outputs`` must be False)."""
+def circuitscape_ini(path, *, write_outputs: bool = False, tol: float = 1e-13, device=None,
+                     _solver=None) -> CircuitscapeResult:
+    """Run a Circuitscape INI file on rasters (scenarios pairwise, advanced, one-to-all and all-to-one), as the
+    reference's ``circuitscape_ini`` does (circuitscape.py:1039-1213); paths are read from the working directory, or
+    else next to the INI file.  ``maps`` are keyed as Circuitscape names its files (``voltmap_<id1>_<id2>``,
+    ``curmap_<id>``...).  Writing output files is not supported (``write_outputs`` must be False).  ``_solver``
+    replaces the GPU solve of the advanced-mode scenarios (a callable with the signature of multi_advanced without
+    its keywords)."""
     if write_outputs:
         raise NotImplementedError("writing Circuitscape output files is not supported")
     path = Path(path)
@@ -943,8 +1384,9 @@ def circuitscape_ini(path, *, write_outputs: bool = False, tol: float = 1e-13, d
     cfg = {**DEFAULTS, **parse_config(path)}
     if cfg["data_type"] not in ("raster", "Raster"):
         raise NotImplementedError(f'data_type = "{cfg["data_type"]}": only rasters are supported')
-    if cfg["scenario"] not in ("pairwise", "Pairwise"):
-        raise NotImplementedError(f'scenario = "{cfg["scenario"]}": only the pairwise scenario is supported')
+    scenario = SCENARIOS.get(cfg["scenario"])
+    if scenario is None:
+        raise ValueError(f'scenario = "{cfg["scenario"]}" is not one of {sorted(set(SCENARIOS.values()))}')
     for key in ("low_memory_mode", "preemptive_memory_release"):
         if cfg.get(key, "False") in TRUELIST:
             raise ValueError(f"{key} is not implemented in Circuitscape.jl; remove it or set it to False")
@@ -968,8 +1410,45 @@ def circuitscape_ini(path, *, write_outputs: bool = False, tol: float = 1e-13, d
         g = g * np.where(m > 0, 1.0, 0.0)
         if g.sum() == 0:
             raise ValueError("Mask file deleted everything!")
+    four = _flag(cfg, "connect_four_neighbors_only")
+    avg = _flag(cfg, "connect_using_avg_resistances")
+    policy = cfg["remove_src_or_gnd"]
+    if policy == "not entered":  # Circuitscape 4's default
+        policy = "keepall"
+    if policy not in POLICIES:
+        raise ValueError(f"remove_src_or_gnd must be one of {POLICIES}")
+    solver = _solver if _solver is not None else (lambda *a: multi_advanced(*a, tol=tol, device=device))
+
+    if scenario == "advanced":
+        src, gnd = _source_and_ground(need("source_file"), need("ground_file"), meta,
+                                      _flag(cfg, "ground_file_is_resistances"))
+        return _advanced(g, poly, src, gnd, four, avg, policy, _flag(cfg, "use_unit_currents"),
+                         _flag(cfg, "use_direct_grounds"), solver)
+
     points = read_point_map(need("point_file"), meta)
     pairs = read_included_pairs(need("included_pairs_file")) if _flag(cfg, "use_included_pairs") else None
+    maps: dict = {}
+    if scenario != "pairwise":
+        strengths = (read_point_strengths(need("variable_source_file"))
+                     if _flag(cfg, "use_variable_source_strengths") else None)
+        cum_only = _flag(cfg, "write_cum_cur_map_only")
+        opts = {"volt_maps": _flag(cfg, "write_volt_maps"),
+                # the advanced-mode kernel writes every point's current map with write_cum_cur_map_only too
+                "cur_maps": _flag(cfg, "write_cur_maps") or cum_only,
+                "cum": _flag(cfg, "write_cur_maps") or cum_only, "max": _flag(cfg, "write_max_cur_maps"),
+                "focal_zero": _flag(cfg, "set_focal_node_currents_to_zero")}
+
+        def emit_point(n, volt, curmap):
+            if volt is not None:
+                maps[f"voltmap_{n}"] = volt
+            if curmap is not None:
+                maps[f"curmap_{n}"] = curmap
+
+        result = _one_to_all(g, poly, points, strengths, pairs, scenario == "one-to-all", four, avg, opts,
+                             emit_point, solver)
+        result.maps = maps
+        return result
+
     points, excluded = _apply_included_pairs(points, pairs)
     cur, cum_only = _flag(cfg, "write_cur_maps"), _flag(cfg, "write_cum_cur_map_only")
     o = PairOptions(volt_maps=_flag(cfg, "write_volt_maps"), cur_maps=cur and not cum_only, cum=cur or cum_only,
@@ -977,7 +1456,6 @@ def circuitscape_ini(path, *, write_outputs: bool = False, tol: float = 1e-13, d
                     null_currents=_flag(cfg, "set_null_currents_to_nodata"),
                     null_voltages=_flag(cfg, "set_null_voltages_to_nodata"),
                     log_transform=_flag(cfg, "log_transform_maps"))
-    maps: dict = {}
     ids = np.unique(points.ids) if points.has_regions else points.ids
 
     def emit(ci, cj, volt, curmap):
@@ -987,6 +1465,5 @@ def circuitscape_ini(path, *, write_outputs: bool = False, tol: float = 1e-13, d
         if curmap is not None:
             maps["curmap" + name] = curmap
 
-    res, cum, mx, stats = _run_pairwise(g, poly, points, excluded, _flag(cfg, "connect_four_neighbors_only"),
-                                        _flag(cfg, "connect_using_avg_resistances"), o, emit, tol, device)
+    res, cum, mx, stats = _run_pairwise(g, poly, points, excluded, four, avg, o, emit, tol, device)
     return CircuitscapeResult(resistances=res, cum_current=cum, max_current=mx, maps=maps, stats=stats)

@@ -10,6 +10,10 @@ Laplacian directly (scipy's sparse LU) where the reference uses its own multifro
 - ``pairwise``: ``raster_pairwise``, ``circuitscape.cpp:474-743`` (jobs, grounding at the component's last node,
   per-pair maps, the shortcut of ``update_voltmatrix!`` / ``update_shortcut_resistances!``);
 - ``region_polymap`` / ``pairwise_regions``: ``circuitscape.cpp:749-866`` (a graph per pair of focal regions);
+- ``node_sums`` / ``resolve`` / ``advanced_many`` / ``multi_advanced``: ``node_sums``, ``resolve`` and
+  ``raster_advanced_many`` (``circuitscape.cpp:382-391,881-1083``) and the native ``circuitscape_multi_advanced``
+  (``src/cpp/circuit/python.cpp:404-480``): advanced-mode problems with direct and finite grounds, solved per
+  component and problem (the reference's Schur-complement shortcut is exact, so a plain solve stands for it);
 - ``pairwise_ini``: the pairwise branch of ``circuitscape_ini``, ``src/landschaft/circuit/circuitscape.py:1039-1170``.
 
 The file parsers (ASCII grids, point lists, pair files) are the package's own; the reference's golden outputs of
@@ -132,8 +136,14 @@ def raster_graph(gmap, polymap, avg_resistances, four_neighbors):
             "degree": np.array(degree), "comp": np.array(comp, dtype=np.int64), "n_comp": n_comp}
 
 
-def node_currents(G, members, v):
-    """graph_node_currents over the nodes `members` (ascending) with voltages v by node."""
+def node_currents(G, members, v, finite=None):
+    """graph_node_currents over the nodes `members` (ascending) with voltages v by node (finite grounds by node
+    or None)."""
+    with np.errstate(divide="ignore", invalid="ignore"):  # b / 0 is +-inf, as in C++
+        return _node_currents(G, members, v, finite)
+
+
+def _node_currents(G, members, v, finite):
     rows = G["rows"]
     maxin = maxout = -math.inf
     for c in members:
@@ -155,6 +165,12 @@ def node_currents(G, members, v):
             elif b < 0:
                 if not (abs(b / maxout) < 1e-8):
                     outflow -= b
+        if finite is not None:
+            f = finite[c] * v[c]
+            if f < 0:
+                inflow -= f
+            elif f > 0:
+                outflow += f
         cur[c] = inflow if inflow > outflow else outflow
     return cur
 
@@ -180,6 +196,98 @@ def _component_solver(G, members, ref):
         return loc, None
     lu = splu(csc_matrix((vals, (ri, ci)), shape=(m, m)))
     return loc, lu
+
+
+def node_sums(G, cells, vals):
+    nx = G["nx"]
+    order = sorted(range(len(cells)), key=lambda k: (cells[k] % nx, cells[k] // nx))
+    s = [0.0] * G["n_nodes"]
+    for k in order:
+        v = G["nodemap"][cells[k]]
+        if v >= 0 and vals[k] != 0:
+            s[v] += vals[k]
+    return s
+
+
+def resolve(src, gnd, policy):
+    n = len(src)
+    src, gnd = list(src), list(gnd)
+    finite = [gnd[v] if gnd[v] < math.inf else 0.0 for v in range(n)]
+    for v in range(n):
+        if not (src[v] != 0 and gnd[v] != 0):
+            continue
+        if policy in ("rmvsrc", "rmvall"):
+            src[v] = 0.0
+        elif policy == "rmvgnd":
+            gnd[v] = 0.0
+    for v in range(n):
+        if gnd[v] == math.inf and src[v] > 0:
+            gnd[v] = 0.0
+    return src, gnd, finite
+
+
+def advanced_many(G, srcs, gnds, only_nodes, policy):
+    from scipy.sparse import csc_matrix
+    from scipy.sparse.linalg import splu
+    n = G["n_nodes"]
+    comp = G["comp"]
+    out = []
+    res = [resolve(s, g, policy) for s, g in zip(srcs, gnds)]
+    for s, g, _ in res:
+        out.append({"voltage": np.zeros(n), "current": np.zeros(n), "solved": False,
+                    "active": np.array([v for v in range(n) if s[v] != 0 or g[v] != 0], dtype=np.int32)})
+    for k in range(G["n_comp"]):
+        members = [v for v in range(n) if comp[v] == k]
+        for p, (s, g, fin) in enumerate(res):
+            only = only_nodes[p]
+            if only == -2 or (only >= 0 and comp[only] != k):
+                continue
+            ss = tt = 0.0
+            for v in members:
+                ss += s[v]
+                tt += g[v]
+            if not (ss != 0 and tt != 0):
+                continue
+            out[p]["solved"] = True
+            unk = [v for v in members if g[v] != math.inf]
+            loc = {v: i for i, v in enumerate(unk)}
+            ri, ci, vals = [], [], []
+            for v in unk:
+                i = loc[v]
+                ri.append(i)
+                ci.append(i)
+                vals.append((G["degree"][v] + fin[v]) + K_SHIFT)
+                for t_, w in G["rows"][v]:
+                    if t_ in loc:
+                        ri.append(i)
+                        ci.append(loc[t_])
+                        vals.append(-w)
+            volt = out[p]["voltage"]
+            if unk:
+                lu = splu(csc_matrix((vals, (ri, ci)), shape=(len(unk), len(unk))))
+                x = lu.solve(np.array([s[v] for v in unk]))
+                for v in unk:
+                    volt[v] = x[loc[v]]
+            cn = node_currents(G, members, volt, fin)
+            for v in members:
+                out[p]["current"][v] = cn[v]
+    return out
+
+
+def multi_advanced(g, poly, avg, four, problems, policy):
+    """circuitscape_multi_advanced: (nodemap as a grid, one result dict per problem)."""
+    G = raster_graph(g, poly, avg, four)
+    srcs, gnds, only = [], [], []
+    for q in problems:
+        srcs.append(node_sums(G, [int(c) for c in q["src_cells"]], [float(v) for v in q["src_vals"]]))
+        gnds.append(node_sums(G, [int(c) for c in q["gnd_cells"]], [float(v) for v in q["gnd_vals"]]))
+        o = -1
+        if q["check_cell"] >= 0:
+            o = int(G["nodemap"][q["check_cell"]])
+            if o < 0:
+                o = -2
+        only.append(o)
+    return G["nodemap"].reshape(g.shape), advanced_many(G, srcs, gnds, only, policy)
 
 
 def pairwise(G, gmap, points, excluded, opts, emit=None):

@@ -12,10 +12,13 @@ landschaft source tree).  Reads the reference's own test data:
   INI runs (the CHOLMOD outputs; the cg+amg outputs are left out);
 * ``tests/data/reference/circuit/circuitscape/input/raster/pairwise/*`` and the
   ``sgVerify*`` entries of ``circuitscape.npz``: Circuitscape's 17 pairwise INI
-  cases (resistance matrices and current / voltage maps).
+  cases (resistance matrices and current / voltage maps);
+* ``.../input/raster/{advanced,one_to_all,all_to_one}/*`` and the ``mgVerify*``,
+  ``ex_advanced``, ``oneToAllVerify*`` and ``allToOneVerify*`` entries: the
+  advanced, one-to-all and all-to-one INI cases.
 
 Writes ``omniscape_golden.npz``, ``advanced_golden.npz``, ``omniscape_ini.npz``,
-``circuitscape/pairwise.npz`` and copies of the INI and input files (same
+``circuitscape/pairwise.npz``, ``circuitscape/modes.npz`` and copies of the INI and input files (same
 layout) next to this file.
 The GPU machines do not have the reference tree, so the tests read only these
 fixtures.
@@ -59,7 +62,10 @@ def main():
     out_dir = HERE / "circuitscape"
     out_dir.mkdir(exist_ok=True)
     np.savez_compressed(out_dir / "pairwise.npz", **{k: z[k] for k in z.files if k.startswith("sgVerify")})
-    for f in sorted((cs / "input" / "raster" / "pairwise").rglob("*")):
+    np.savez_compressed(out_dir / "modes.npz", **{k: z[k] for k in z.files
+                                                 if k.startswith(("mgVerify", "ex_advanced", "oneToAll", "allToOne"))})
+    sub = ("pairwise", "advanced", "one_to_all", "all_to_one")
+    for f in sorted(x for s in sub for x in (cs / "input" / "raster" / s).rglob("*")):
         if f.is_file():
             dst = out_dir / f.relative_to(cs)
             dst.parent.mkdir(parents=True, exist_ok=True)

@@ -132,8 +132,14 @@ def test_region_polymap_matches_the_oracle():
 
 def test_ini_errors(tmp_path):
     ini = tmp_path / "a.ini"
-    ini.write_text("[Options]\nscenario = one-to-all\n")
+    ini.write_text("[Options]\nscenario = one-to-many\n")
+    with pytest.raises(ValueError, match="scenario"):
+        cs.circuitscape_ini(ini)
+    ini.write_text("[Options]\ndata_type = network\nscenario = pairwise\n")
     with pytest.raises(NotImplementedError):
+        cs.circuitscape_ini(ini)
+    ini.write_text("[Options]\nscenario = advanced\nremove_src_or_gnd = rmvsome\n")
+    with pytest.raises(ValueError):
         cs.circuitscape_ini(ini)
     ini.write_text("[Options]\nscenario = pairwise\nuse_polygons = maybe\nhabitat_file = x.asc\n")
     with pytest.raises(FileNotFoundError):
@@ -161,3 +167,75 @@ def test_graph_abi_argument_checks():
     rc = lib.lsb_graph_pairs(5, None, None, None, None, 0, 2, None, None, C.byref(p), None, None, None, 0,
                              C.byref(st), err, len(err), None)
     assert rc == N.LSB_ERR_ARGUMENT
+
+
+# --- advanced, one-to-all and all-to-one ---------------------------------------------------------------------------
+
+def _mode_cases(scenario):
+    return sorted(str(p.relative_to(CS)) for p in (CS / "input" / "raster" / scenario).glob("*/*.ini"))
+
+
+ADVANCED_CASES = _mode_cases("advanced")
+ONE_TO_ALL_CASES = _mode_cases("one_to_all")
+ALL_TO_ONE_CASES = _mode_cases("all_to_one")
+
+
+def check_advanced(name, r, rtol=1e-9):
+    """The reference's bar for advanced mode: zero pattern equal, values within rtol (atol 1e-11 of the largest)."""
+    z = np.load(CS / "modes.npz")
+    checked = 0
+    for key, ours in (("voltmap.asc", r.voltage), ("curmap.asc", r.current), ("result.txt", r.voltage)):
+        k = f"{name}/{key}"
+        if k not in z.files:
+            continue
+        ref = z[k]
+        np.testing.assert_array_equal(ours == 0, ref == 0)
+        np.testing.assert_allclose(ours, ref, rtol=rtol, atol=1e-11 * np.abs(ref).max())
+        checked += 1
+    assert checked >= 2
+
+
+def check_one_to_all(name, r, rtol=1e-11):
+    """The reference's bar for one-to-all / all-to-one (rtol 1e-11 with a direct solver)."""
+    z = np.load(CS / "modes.npz")
+    np.testing.assert_allclose(r.resistances, z[f"{name}/result.txt"], rtol=rtol, atol=rtol * 1e-2)
+    for key, ours in (("cum_curmap.asc", r.cum_current), ("max_curmap.asc", r.max_current)):
+        if f"{name}/{key}" in z.files:
+            want = z[f"{name}/{key}"]
+            np.testing.assert_allclose(ours, want, rtol=rtol, atol=rtol * 0.1 * np.abs(want).max())
+    theirs = {k.split("/")[1][:-4] for k in z.files if k.startswith(name + "/")
+              and k.split("/")[1].startswith(("curmap_", "voltmap_"))}
+    assert set(r.maps) == theirs
+    for kind in theirs:
+        want = z[f"{name}/{kind}.asc"]
+        np.testing.assert_allclose(r.maps[kind], want, rtol=rtol, atol=rtol * 0.1 * max(np.abs(want).max(), 1e-300))
+
+
+@pytest.mark.parametrize("ini", ADVANCED_CASES)
+def test_oracle_matches_circuitscape_advanced(ini, in_cs):
+    check_advanced(Path(ini).stem, cs.circuitscape_ini(ini, _solver=O.multi_advanced))
+
+
+@pytest.mark.parametrize("ini", ONE_TO_ALL_CASES + ALL_TO_ONE_CASES)
+def test_oracle_matches_circuitscape_one_to_all(ini, in_cs):
+    check_one_to_all(Path(ini).stem, cs.circuitscape_ini(ini, _solver=O.multi_advanced))
+
+
+def test_mode_case_counts():
+    assert (len(ADVANCED_CASES), len(ONE_TO_ALL_CASES), len(ALL_TO_ONE_CASES)) == (8, 13, 12)
+
+
+@pytest.mark.parametrize("policy", cs.POLICIES)
+def test_node_sums_and_conflicts_match_the_oracle(policy):
+    rng = np.random.default_rng(3)
+    g, poly = random_case(rng, 11, 9, True)
+    graph = cs.raster_graph(g, poly, False, False)
+    G = O.raster_graph(g, poly, False, False)
+    cells = rng.integers(0, g.size, 30)
+    vals = rng.normal(size=30)
+    vals[::5] = 0.0
+    np.testing.assert_array_equal(cs.node_sums(graph, cells, vals), O.node_sums(G, list(cells), list(vals)))
+    src = np.where(rng.random(graph.n_nodes) < 0.3, rng.normal(size=graph.n_nodes), 0.0)
+    gnd = np.where(rng.random(graph.n_nodes) < 0.3, rng.choice([0.5, 2.0, np.inf], graph.n_nodes), 0.0)
+    for a, b in zip(cs.resolve_conflicts(src, gnd, policy), O.resolve(list(src), list(gnd), policy)):
+        np.testing.assert_array_equal(a, np.array(b))

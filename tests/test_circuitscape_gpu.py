@@ -16,7 +16,8 @@ ROOT = Path(__file__).resolve().parents[1]
 sys.path.insert(0, str(ROOT / "tests"))
 sys.path.insert(0, str(ROOT / "oracle"))
 import circuitscape_oracle as O  # noqa: E402
-from test_circuitscape_cpu import (CS, POINT_CASES, REGION_CASES, check_against_golden, ini_path,  # noqa: E402
+from test_circuitscape_cpu import (ADVANCED_CASES, ALL_TO_ONE_CASES, CS, ONE_TO_ALL_CASES, POINT_CASES,  # noqa
+                                   REGION_CASES, check_advanced, check_against_golden, check_one_to_all, ini_path,
                                    random_case)
 
 pytestmark = pytest.mark.gpu
@@ -209,3 +210,102 @@ def test_iteration_cap_reports_failure():
     p = N.default_graph_params()
     rc, _, _, st, _ = solve_path([1.0] * 30, 30, [0, 40], [15, 3], p)  # a node index out of range fails that job
     assert rc == N.LSB_ERR_NOT_CONVERGED and st.failures == 1
+
+
+# --- advanced, one-to-all and all-to-one (lsb_graph_solve) ---------------------------------------------------------
+
+@pytest.mark.parametrize("ini", ADVANCED_CASES)
+def test_advanced_matches_circuitscape(ini, in_cs):
+    check_advanced(Path(ini).stem, cs.circuitscape_ini(ini))  # the reference's bar, rtol 1e-9
+
+
+@pytest.mark.parametrize("ini", ONE_TO_ALL_CASES + ALL_TO_ONE_CASES)
+def test_one_to_all_matches_circuitscape(ini, in_cs):
+    # the reference's bar is 1e-11 for its direct solver; the GPU's iterative solve is held to 1e-9
+    check_one_to_all(Path(ini).stem, cs.circuitscape_ini(ini), rtol=1e-9)
+
+
+@pytest.mark.parametrize("policy", cs.POLICIES)
+def test_random_advanced_matches_the_oracle(policy):
+    rng = np.random.default_rng(40 + cs.POLICIES.index(policy))
+    ny, nx = 23, 19
+    g, poly = random_case(rng, ny, nx, True)
+    src = np.where(rng.random((ny, nx)) < 0.05, rng.normal(size=(ny, nx)), 0.0)
+    gnd = np.where(rng.random((ny, nx)) < 0.05, rng.choice([0.0, 0.3, 4.0], (ny, nx)), cs.NODATA)
+    kw = dict(habitat_is_resistance=False, polygons=poly, remove_src_or_gnd=policy)
+    r = cs.circuitscape_advanced(g, src, gnd, **kw)
+    gr = np.where(gnd == cs.NODATA, 0.0, np.divide(1.0, gnd, out=np.full_like(gnd, np.inf), where=gnd != 0))
+    want = cs._advanced(g, poly, src, gr, False, False, policy, False, False, O.multi_advanced)
+    assert r.maps["solved"] == want.maps["solved"]
+    np.testing.assert_array_equal(r.nodemap, want.nodemap)
+    for ours, ref in ((r.voltage, want.voltage), (r.current, want.current)):
+        np.testing.assert_allclose(ours, ref, rtol=1e-9, atol=1e-11 * max(np.abs(ref).max(), 1e-300))
+
+
+@pytest.mark.parametrize("all_to_one", [False, True])
+def test_one_to_all_api_matches_the_oracle(all_to_one):
+    rng = np.random.default_rng(50 + all_to_one)
+    ny, nx = 20, 24
+    g, poly = random_case(rng, ny, nx, True)
+    pm = np.zeros((ny, nx))
+    pm.flat[rng.choice(ny * nx, size=6, replace=False)] = np.arange(1, 7)
+    flags = dict(habitat_is_resistance=False, polygons=poly, voltage_maps=True, current_maps=True, max_map=True)
+    r = cs.circuitscape_one_to_all(g, pm, all_to_one=all_to_one, **flags)
+    maps = {}
+
+    def emit(n, volt, cur):
+        if volt is not None:
+            maps[("voltage", n)] = volt
+        if cur is not None:
+            maps[("current", n)] = cur
+
+    opts = {"volt_maps": True, "cur_maps": True, "cum": True, "max": True, "focal_zero": False}
+    want = cs._one_to_all(g, poly, cs._points_from_map(pm), None, None, not all_to_one, False, False, opts, emit,
+                          O.multi_advanced)
+    np.testing.assert_allclose(r.resistances, want.resistances, rtol=1e-9, atol=1e-12)
+    scale = np.abs(want.cum_current).max()
+    np.testing.assert_allclose(r.cum_current, want.cum_current, rtol=1e-9, atol=1e-11 * scale)
+    np.testing.assert_allclose(r.max_current, want.max_current, rtol=1e-9, atol=1e-11 * scale)
+    assert set(r.maps) == set(maps)
+    for k, v in maps.items():
+        np.testing.assert_allclose(r.maps[k], v, rtol=1e-9, atol=1e-11 * max(np.abs(v).max(), 1e-300))
+
+
+def test_graph_solve_closed_form():
+    # a path 0 - 1 - 2 - 3 with conductances w: a unit source at 0 and a finite ground of conductance 0.5 at 3
+    # (voltages sum 1/w + 1/0.5 down the path); a second job with a direct ground at 3 instead
+    import torch
+    lib = N.load()
+    w = [2.0, 0.5, 4.0]
+    n = 4
+    adj, wt, ptr = [], [], [0]
+    for i in range(n):
+        for k in (i - 1, i + 1):
+            if 0 <= k < n:
+                adj.append(k)
+                wt.append(w[min(i, k)])
+        ptr.append(len(adj))
+    diag = np.array([sum(wt[ptr[i]:ptr[i + 1]]) for i in range(n)]) + cs.K_SHIFT
+    dev = torch.device("cuda", 0)
+    t = lambda a, dt: torch.tensor(np.asarray(a), dtype=dt, device=dev)  # noqa: E731
+    args = [t(ptr, torch.int64), t(adj, torch.int32), t(wt, torch.float64), t(diag, torch.float64)]
+    lists = [t([0, 1, 2], torch.int64), t([0, 0], torch.int32), t([1.0, 1.0], torch.float64),
+             t([0, 0, 1], torch.int64), t([3], torch.int32), t([0, 1, 1], torch.int64), t([3], torch.int32),
+             t([0.5], torch.float64)]
+    volt = torch.empty((2, n), dtype=torch.float64, device=dev)
+    cur = torch.empty_like(volt)
+    p = N.default_graph_params()
+    nb = C.c_size_t(0)
+    assert lib.lsb_graph_solve_workspace_size(n, 2, C.byref(p), C.byref(nb)) == 0
+    ws = torch.empty(nb.value, dtype=torch.uint8, device=dev)
+    st = N.GraphStats()
+    err = C.create_string_buffer(256)
+    rc = lib.lsb_graph_solve(n, *(a.data_ptr() for a in args), 2, *(a.data_ptr() for a in lists), C.byref(p),
+                             volt.data_ptr(), cur.data_ptr(), ws.data_ptr(), nb.value, C.byref(st), err, len(err),
+                             torch.cuda.current_stream().cuda_stream)
+    assert rc == 0 and st.failures == 0, err.value
+    v, c = volt.cpu().numpy(), cur.cpu().numpy()
+    np.testing.assert_allclose(v[0], [1 / 2 + 1 / 0.5 + 1 / 4 + 2, 1 / 0.5 + 1 / 4 + 2, 1 / 4 + 2, 2], rtol=1e-12)
+    np.testing.assert_allclose(c[0], np.ones(4), rtol=1e-12)  # the finite ground's current counts at node 3
+    np.testing.assert_allclose(v[1], [1 / 2 + 1 / 0.5 + 1 / 4, 1 / 0.5 + 1 / 4, 1 / 4, 0.0], rtol=1e-12, atol=1e-15)
+    np.testing.assert_allclose(c[1], np.ones(4), rtol=1e-12)
