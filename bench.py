@@ -252,9 +252,12 @@ PW_METRIC = "Circuitscape pairwise: pair solves/s (unit current between two foca
 
 def bench_pairwise(args, rank, world, local, d):
     """Circuitscape's pairwise mode with current maps on a 256 x 256 raster with 24 focal points (276 pairs, every
-    pair solved); a step is one lsb_graph_pairs call over all pairs of the component (device-resident system)."""
+    pair solved).  The graph is a plain grid, so the pairs run on the raster solver (as circuitscape_pairwise routes
+    them): a step is one lsb_rasters call over the 276 pair rasters (unit source at the pair's destination, direct
+    ground at its source), inputs resident on the device.  The node-graph kernel (lsb_graph_pairs, Jacobi CG) is
+    timed beside it over the same pairs."""
     import torch
-    from landschaft_b200 import circuitscape as cs, synthetic
+    from landschaft_b200 import circuitscape as cs, raster as RA, synthetic
     r, pm = synthetic.pairwise_256(rank)
     dev = torch.device("cuda", local)
     g = cs.habitat_conductance(np.where(np.isnan(r), cs.NODATA, r))
@@ -272,10 +275,30 @@ def bench_pairwise(args, rank, world, local, d):
     src = torch.tensor([int(sys_.local[nodes[a]]) for a, _ in pairs], dtype=torch.int32, device=dev)
     dst = torch.tensor([int(sys_.local[nodes[b]]) for _, b in pairs], dtype=torch.int32, device=dev)
     n, nj = len(members), len(pairs)
-    _, _, st = cs.solve_pairs(dsys, ground, src, dst)
+    if args.profile_run:  # the first 96 pairs in one call (their vectors, 200 MB, exceed L2)
+        _, _, st = cs.solve_pairs(dsys, ground, src[:96], dst[:96])
+        print(json.dumps({"profile_run": "pairwise_256 (first 96 pairs)", "nodes": n,
+                          "cg_iterations_mean": st.iters_mean}), flush=True)
+        d.close()
+        return
+    # the raster route: one packed batch of pair rasters
+    assert cs.raster_route(graph)
+    ncell = g.size
+    on = np.flatnonzero(graph.nodemap >= 0)
+    node_cell = np.empty(graph.n_nodes, dtype=np.int64)
+    node_cell[graph.nodemap[on]] = on
+    base = np.arange(nj, dtype=np.int64) * ncell
+    G = torch.from_numpy(np.ascontiguousarray(g).ravel()).to(dev).repeat(nj)
+    S = torch.zeros(nj * ncell, dtype=torch.float64, device=dev)
+    GR = torch.zeros_like(S)
+    S[torch.from_numpy(base + node_cell[[nodes[b] for _, b in pairs]]).to(dev)] = 1.0
+    GR[torch.from_numpy(base + node_cell[[nodes[a] for a, _ in pairs]]).to(dev)] = np.inf
+    rp = RA.raster_params(four_neighbors=False, tol=1e-12)
+    shapes = [g.shape] * nj
+    _, _, rst = RA.run_rasters(G, S, GR, shapes, rp)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     for _ in range(args.warmup):
-        cs.solve_pairs(dsys, ground, src, dst, stats=False)
+        RA.run_rasters(G, S, GR, shapes, rp, want_stats=False)
     clocks = Clocks(local)
     d.barrier()
     torch.cuda.synchronize()
@@ -285,13 +308,22 @@ def bench_pairwise(args, rank, world, local, d):
         flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        cs.solve_pairs(dsys, ground, src, dst, stats=False)
+        RA.run_rasters(G, S, GR, shapes, rp, want_stats=False)
         e1.record()
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1) / 1e3)
     clk = clocks.stop()
     d.barrier()
     T = d.max(sum(times))
+    # the node-graph kernel over the same pairs (one timed call after one untimed)
+    _, _, st = cs.solve_pairs(dsys, ground, src, dst)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    cs.solve_pairs(dsys, ground, src, dst, stats=False)
+    e1.record()
+    torch.cuda.synchronize()
+    t_graph = d.max(e0.elapsed_time(e1) / 1e3)
     # end to end: the public call from host rasters (graph, solves, maps)
     te = []
     for _ in range(max(1, min(args.steps, 2))):
@@ -328,14 +360,17 @@ def bench_pairwise(args, rank, world, local, d):
     if rank == 0:
         line = {"metric": PW_METRIC, "value": world * nj * args.steps / T, "unit": "pairs/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * T / args.steps,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 CG + f64 refinement",
                 "data": "synthetic (seeded Gaussian random field, 24 random focal points)",
                 "config": {"workload": "pairwise_256", "nodes": n, "pairs": nj, "neighbours": 8,
-                           "l2": "flushed between timed steps (256 MiB write)", "tol": 1e-14},
+                           "l2": "flushed between timed steps (256 MiB write)", "tol": 1e-12},
                 "e2e": {"value": world * nj / TE, "unit": "pairs/s", "h2d_bytes_per_step": int(2 * 8 * g.size),
                         "d2h_bytes_per_step": int(nj * 2 * 8 * n), "includes": "host graph build and map assembly"},
-                "cg_iterations": {"mean": st.iters_mean, "max": st.iters_max}, "ctas": st.ctas,
-                "worst_residual": st.worst_residual, "max_rel_err_vs_oracle": err, "clocks": clk,
+                "solver": "lsb_rasters (FP32 CG, multigrid, FP64 refinement to 1e-12)",
+                "cg_iterations": {"mean": rst.iters_total / max(rst.n_solved, 1), "max": rst.iters_max},
+                "graph_kernel": {"value": world * nj / t_graph, "unit": "pairs/s", "kernel": "lsb_graph_pairs",
+                                 "cg_iterations_mean": st.iters_mean, "ctas": st.ctas,
+                                 "worst_residual": st.worst_residual}, "max_rel_err_vs_oracle": err, "clocks": clk,
                 "gpu_launches": args.steps, "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
     d.close()

@@ -308,6 +308,9 @@ class RasterGraph:
     degree: np.ndarray    # float64
     comp: np.ndarray      # node -> component
     n_comp: int
+    four_neighbors: bool = False
+    avg_resistances: bool = False
+    merged: bool = False  # a node covers several cells, or a cell without habitat
 
 
 def _average(x, y, diagonal: bool, resistances: bool):
@@ -393,8 +396,9 @@ def raster_graph(gmap: np.ndarray, polymap: np.ndarray | None, avg_resistances: 
         rows = np.flatnonzero(ptr[:-1] + k < ptr[1:])
         degree[rows] += wsum[ptr[:-1][rows] + k]
     comp, n_comp = _components(n_nodes, ptr, B, wsum)
+    merged = bool(np.count_nonzero(nodemap >= 0) != n_nodes or np.any((nodemap >= 0) & ~(g > 0)))
     return RasterGraph(nx, ny, n_nodes, nodemap, ptr, B.astype(np.int32), wsum.astype(np.float64), degree, comp,
-                       n_comp)
+                       n_comp, bool(four_neighbors), bool(avg_resistances), merged)
 
 
 def _components(n_nodes, ptr, adj, w):
@@ -522,6 +526,56 @@ def _solve_component(graph: RasterGraph, members: np.ndarray, ground: int, src: 
     return volt, cur
 
 
+MAX_RASTER_SIDE = 1024  # the raster solver's limit
+
+
+def raster_route(graph: RasterGraph) -> bool:
+    """Whether the pair solves can run on the raster solver: a plain grid graph (one habitat cell per node, no
+    short-circuit regions), average-conductance weights and sides within the raster solver's limit."""
+    return (not graph.merged and not graph.avg_resistances and graph.nx <= MAX_RASTER_SIDE
+            and graph.ny <= MAX_RASTER_SIDE)
+
+
+def _solve_component_rasters(graph: RasterGraph, gmap: np.ndarray, members: np.ndarray, src: np.ndarray,
+                             dst: np.ndarray, want_currents: bool, tol: float, stats: GraphSolveStats, device):
+    """The jobs of one component on the raster solver (lsb_rasters: FP32 CG with a multigrid preconditioner inside
+    FP64 refinement): job j is the raster with a unit source at dst[j]'s cell and a direct ground at src[j]'s, whose
+    voltages are the pair's voltages relative to its source and whose node currents are the pair's.  Same contract
+    as _solve_component."""
+    import torch
+
+    from . import raster as R
+    ny, nx = graph.ny, graph.nx
+    ncell = nx * ny
+    on = np.flatnonzero(graph.nodemap >= 0)
+    node_cell = np.empty(graph.n_nodes, dtype=np.int64)
+    node_cell[graph.nodemap[on]] = on
+    mcell = torch.from_numpy(node_cell[members]).to(device)
+    nj = len(src)
+    volt = np.empty((nj, len(members)))
+    cur = np.empty((nj, len(members))) if want_currents else None
+    p = R.raster_params(four_neighbors=graph.four_neighbors, tol=tol)
+    g_dev = torch.from_numpy(np.ascontiguousarray(gmap, dtype=np.float64).ravel()).to(device)
+    per = max(1, min(nj, (1 << 31) // (40 * ncell)))  # inputs and outputs of a batch within 2 GiB
+    for b0 in range(0, nj, per):
+        b1 = min(nj, b0 + per)
+        nb = b1 - b0
+        base = torch.arange(nb, device=device, dtype=torch.int64) * ncell
+        S = torch.zeros(nb * ncell, dtype=torch.float64, device=device)
+        GR = torch.zeros_like(S)
+        S[base + torch.from_numpy(node_cell[dst[b0:b1]]).to(device)] = 1.0
+        GR[base + torch.from_numpy(node_cell[src[b0:b1]]).to(device)] = np.inf
+        c, v, st = R.run_rasters(g_dev.repeat(nb), S, GR, [(ny, nx)] * nb, p)
+        volt[b0:b1] = v.view(nb, ncell)[:, mcell].cpu().numpy()
+        if want_currents:
+            cur[b0:b1] = c.view(nb, ncell)[:, mcell].cpu().numpy()
+        mean = st.iters_total / max(st.n_solved, 1)
+        stats.iters_mean = (stats.iters_mean * stats.jobs + mean * nb) / (stats.jobs + nb)
+        stats.jobs += nb
+        stats.iters_max = max(stats.iters_max, int(st.iters_max))
+    return volt, cur
+
+
 def graph_params(tol=1e-13, max_iter=0):
     p = N.default_graph_params()
     p.tol = float(tol)
@@ -548,15 +602,23 @@ class PairOptions:
 
 
 def raster_pairwise(graph: RasterGraph, gmap: np.ndarray, points: np.ndarray, excluded: np.ndarray,
-                    o: PairOptions, emit=None, *, tol=1e-13, device=None, stats: GraphSolveStats | None = None):
+                    o: PairOptions, emit=None, *, tol=1e-13, device=None, stats: GraphSolveStats | None = None,
+                    pair_solver: str = "auto"):
     """Effective resistances between the focal points' nodes ``points`` (-1: off the graph), with the pair maps.
 
     Returns ``(resistances n x n, cum, max)``; ``emit(ci, cj, voltage_map, current_map)`` receives each pair's maps
     (None where not asked for).  Follows circuitscape.cpp:474-743: components in order, distinct focal nodes in
     first-appearance order, the component's last node grounded, jobs (source, destination) solved with a unit
     current, and without maps or exclusions the shortcut (only the first focal node's pairs, the others from the
-    voltages)."""
+    voltages).  ``pair_solver``: "graph" (lsb_graph_pairs, any graph), "raster" (lsb_rasters, plain grid graphs) or
+    "auto" (the raster solver where the graph allows it)."""
     import torch
+    if pair_solver not in ("auto", "graph", "raster"):
+        raise ValueError('pair_solver must be "auto", "graph" or "raster"')
+    if pair_solver == "raster" and not raster_route(graph):
+        raise ValueError("the raster pair solver needs a plain grid graph (no short-circuit regions, average "
+                         f"conductances, sides up to {MAX_RASTER_SIDE})")
+    on_rasters = pair_solver == "raster" or (pair_solver == "auto" and raster_route(graph))
     dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
     params = graph_params(tol)
     stats = stats if stats is not None else GraphSolveStats()
@@ -600,7 +662,11 @@ def raster_pairwise(graph: RasterGraph, gmap: np.ndarray, points: np.ndarray, ex
         ground = int(members[-1])
         src = np.array([j[0] for j in jobs], dtype=np.int64)
         dst = np.array([j[1] for j in jobs], dtype=np.int64)
-        volt, cur = _solve_component(graph, members, ground, src, dst, o.maps(), params, stats, dev)
+        if on_rasters:
+            volt, cur = _solve_component_rasters(graph, gmap, members, src, dst, o.maps(), min(tol, 1e-12), stats,
+                                                 dev)
+        else:
+            volt, cur = _solve_component(graph, members, ground, src, dst, o.maps(), params, stats, dev)
         mindex = {int(v): q for q, v in enumerate(members)}
         in_k = cell_comp == k
         cells_k = np.flatnonzero(in_k)
@@ -750,7 +816,8 @@ def region_polymap(polymap, n: int, cells: np.ndarray, ids: np.ndarray, pt1: int
     return poly
 
 
-def _run_regions(g, poly, points: FocalPoints, excluded_ids: set, four, avg, o: PairOptions, emit, tol, device):
+def _run_regions(g, poly, points: FocalPoints, excluded_ids: set, four, avg, o: PairOptions, emit, tol, device,
+                 pair_solver="auto"):
     """pairwise_regions (circuitscape.cpp:781-866): every pair of distinct ids gets its own graph, its two regions
     made short-circuit regions, and one solve between the nodes of their first cells."""
     rows, cols = points.cells
@@ -779,7 +846,7 @@ def _run_regions(g, poly, points: FocalPoints, excluded_ids: set, four, avg, o: 
             got = []
             r2, c2, m2 = raster_pairwise(graph, g, nodes, np.zeros((2, 2), dtype=bool), o,
                                          lambda ci, cj, v, c: got.append((ci, cj, v, c)), tol=tol, device=device,
-                                         stats=stats)
+                                         stats=stats, pair_solver=pair_solver)
             R[i, j] = R[j, i] = r2[0, 1]
             if cum is not None:
                 cum += c2
@@ -798,9 +865,10 @@ def _run_regions(g, poly, points: FocalPoints, excluded_ids: set, four, avg, o: 
     return res, cum, mx, stats
 
 
-def _run_pairwise(g, poly, points: FocalPoints, excluded_ids: set, four, avg, o: PairOptions, emit, tol, device):
+def _run_pairwise(g, poly, points: FocalPoints, excluded_ids: set, four, avg, o: PairOptions, emit, tol, device,
+                  pair_solver="auto"):
     if points.has_regions:
-        return _run_regions(g, poly, points, excluded_ids, four, avg, o, emit, tol, device)
+        return _run_regions(g, poly, points, excluded_ids, four, avg, o, emit, tol, device, pair_solver)
     graph = raster_graph(g, poly, avg, four)
     rows, cols = points.cells
     cells = rows * g.shape[1] + cols
@@ -814,7 +882,8 @@ def _run_pairwise(g, poly, points: FocalPoints, excluded_ids: set, four, avg, o:
             for b in range(n):
                 ex[a, b] = (int(ids[a]), int(ids[b])) in excluded_ids
     stats = GraphSolveStats()
-    R, cum, mx = raster_pairwise(graph, g, nodes, ex, o, emit, tol=tol, device=device, stats=stats)
+    R, cum, mx = raster_pairwise(graph, g, nodes, ex, o, emit, tol=tol, device=device, stats=stats,
+                                 pair_solver=pair_solver)
     res = np.zeros((n + 1, n + 1))
     res[0, 1:] = ids
     res[1:, 0] = ids
@@ -828,7 +897,7 @@ def circuitscape_pairwise(habitat, points, *, habitat_is_resistance: bool = True
                           max_map: bool = False, set_focal_node_currents_to_zero: bool = False,
                           set_null_currents_to_nodata: bool = False, set_null_voltages_to_nodata: bool = False,
                           log_transform_maps: bool = False, reclass: dict | None = None, n_threads: int = 0,
-                          tol: float = 1e-13, device=None) -> CircuitscapeResult:
+                          tol: float = 1e-13, device=None, pair_solver: str = "auto") -> CircuitscapeResult:
     """Effective resistances between every pair of focal points on a raster (drop-in for
     ``ls.circuit.circuitscape_pairwise``, circuitscape.py:550-670), solved on the GPU.
 
@@ -837,7 +906,8 @@ def circuitscape_pairwise(habitat, points, *, habitat_is_resistance: bool = True
     positive are removed; ``included_pairs``: :class:`IncludedPairs` or a path.  The map options keep each pair's
     voltage / current map in ``result.maps`` (keys ``("voltage", id1, id2)`` / ``("current", id1, id2)``) and the
     sum / maximum of the current maps.  ``n_threads`` is accepted for compatibility; ``tol`` is the CG's relative
-    residual target.
+    residual target; ``pair_solver`` chooses the GPU solve of the pairs: "raster" (the multigrid raster solver, for
+    plain grid graphs), "graph" (Jacobi CG on the node graph, any graph) or "auto".
     """
     del n_threads
     cells = _grid(habitat, "habitat")
@@ -881,7 +951,7 @@ def circuitscape_pairwise(habitat, points, *, habitat_is_resistance: bool = True
             maps[("current", *key)] = cur
 
     res, cum, mx, stats = _run_pairwise(g, poly, points, excluded, four_neighbors, avg_resistances, o, emit, tol,
-                                        device)
+                                        device, pair_solver)
     return CircuitscapeResult(resistances=res, cum_current=cum, max_current=mx, maps=maps, stats=stats)
 
 
@@ -1370,7 +1440,7 @@ def _resolve(name: str, base: Path) -> Path:
 
 
 def circuitscape_ini(path, *, write_outputs: bool = False, tol: float = 1e-13, device=None,
-                     _solver=None) -> CircuitscapeResult:
+                     pair_solver: str = "auto", _solver=None) -> CircuitscapeResult:
     """Run a Circuitscape INI file on rasters (scenarios pairwise, advanced, one-to-all and all-to-one), as the
     reference's ``circuitscape_ini`` does (circuitscape.py:1039-1213); paths are read from the working directory, or
     else next to the INI file.  ``maps`` are keyed as Circuitscape names its files (``voltmap_<id1>_<id2>``,
@@ -1465,5 +1535,5 @@ def circuitscape_ini(path, *, write_outputs: bool = False, tol: float = 1e-13, d
         if curmap is not None:
             maps["curmap" + name] = curmap
 
-    res, cum, mx, stats = _run_pairwise(g, poly, points, excluded, four, avg, o, emit, tol, device)
+    res, cum, mx, stats = _run_pairwise(g, poly, points, excluded, four, avg, o, emit, tol, device, pair_solver)
     return CircuitscapeResult(resistances=res, cum_current=cum, max_current=mx, maps=maps, stats=stats)

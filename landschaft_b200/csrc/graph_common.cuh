@@ -16,8 +16,10 @@
 namespace lsbg {
 namespace {
 
-constexpr int kThreads = 256;
-constexpr int kWarps = kThreads / 32;
+// Threads per CTA: 512 (two CTAs per SM) for components of at least kWideNodes nodes, else 256 (four per SM).
+constexpr int kWideNodes = 8192;
+inline int threads_for(int64_t n) { return n >= kWideNodes ? 512 : 256; }
+inline int ctas_per_sm(int nt) { return nt == 512 ? 2 : 4; }
 constexpr int kMaxRestarts = 64;
 constexpr size_t kAlign = 256;
 constexpr double kScratchCap = 8.0 * 1024 * 1024 * 1024;  // bytes of per-CTA vectors at most
@@ -41,6 +43,7 @@ static_assert(sizeof(JobStat) == 16, "JobStat layout");
 
 // Sum of (a, b) over the block, the same value in every thread: warp butterflies, then the warps' partial sums
 // added in warp order.  The leading barrier lets a previous call's readers finish with `red`.
+template <int NT>
 __device__ __forceinline__ double2 block_sum2(double a, double b, double2 *red) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -52,13 +55,14 @@ __device__ __forceinline__ double2 block_sum2(double a, double b, double2 *red) 
     __syncthreads();
     double2 s = red[0];
 #pragma unroll
-    for (int i = 1; i < kWarps; ++i) {
+    for (int i = 1; i < NT / 32; ++i) {
         s.x += red[i].x;
         s.y += red[i].y;
     }
     return s;
 }
 
+template <int NT>
 __device__ __forceinline__ double2 block_max2(double a, double b, double2 *red) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -71,7 +75,7 @@ __device__ __forceinline__ double2 block_max2(double a, double b, double2 *red) 
     __syncthreads();
     double2 s = red[0];
 #pragma unroll
-    for (int i = 1; i < kWarps; ++i) {
+    for (int i = 1; i < NT / 32; ++i) {
         s.x = red[i].x > s.x ? red[i].x : s.x;
         s.y = red[i].y > s.y ? red[i].y : s.y;
     }

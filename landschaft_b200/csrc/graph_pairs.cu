@@ -34,8 +34,9 @@ struct GArgs {
 
 // y = A v on the unknowns (the ground's row is 0; v at the ground is 0).  Entries whose column is out of range are
 // skipped and counted in `bad`.
+template <int NT>
 __device__ __forceinline__ void spmv(const GArgs &a, const double *v, double *y, int &bad) {
-    for (int i = threadIdx.x; i < a.n; i += kThreads) {
+    for (int i = threadIdx.x; i < a.n; i += NT) {
         double s = 0.0;
         if (i != a.ground) {
             s = a.diag[i] * v[i];
@@ -58,11 +59,12 @@ __device__ __forceinline__ double rhs(const GArgs &a, int i, int s, int d) {
     return (i == d ? 1.0 : 0.0) - (i == s ? 1.0 : 0.0);
 }
 
+template <int NT>
 __device__ void solve_job(const GArgs &a, int64_t j, double *r, double *p, double *q, double2 *red) {
     const int n = a.n, s = a.src[j], d = a.dst[j];
     double *x = a.volt + static_cast<size_t>(j) * n;
     if (s < 0 || s >= n || d < 0 || d >= n) {
-        for (int i = threadIdx.x; i < n; i += kThreads) {
+        for (int i = threadIdx.x; i < n; i += NT) {
             x[i] = 0.0;
             if (a.cur) a.cur[static_cast<size_t>(j) * n + i] = 0.0;
         }
@@ -72,7 +74,7 @@ __device__ void solve_job(const GArgs &a, int64_t j, double *r, double *p, doubl
     int bad = 0;
     // x = 0, r = b, p = D^-1 r
     double pr = 0.0, pz = 0.0;
-    for (int i = threadIdx.x; i < n; i += kThreads) {
+    for (int i = threadIdx.x; i < n; i += NT) {
         const double b = rhs(a, i, s, d);
         x[i] = 0.0;
         r[i] = b;
@@ -80,7 +82,7 @@ __device__ void solve_job(const GArgs &a, int64_t j, double *r, double *p, doubl
         pr += b * b;
         pz += b * b / a.diag[i];
     }
-    double2 t = block_sum2(pr, pz, red);
+    double2 t = block_sum2<NT>(pr, pz, red);
     const double bb = t.x;
     double rr = t.x, rz = t.y;
     const double goal = a.tol * a.tol * bb;
@@ -88,42 +90,42 @@ __device__ void solve_job(const GArgs &a, int64_t j, double *r, double *p, doubl
     int it = 0, stall = 0;
     for (int cycle = 0; cycle < kMaxRestarts; ++cycle) {
         while (it < a.max_iter && rr > goal) {
-            spmv(a, p, q, bad);
+            spmv<NT>(a, p, q, bad);
             __syncthreads();
             double ppq = 0.0;
-            for (int i = threadIdx.x; i < n; i += kThreads) ppq += p[i] * q[i];
-            const double pq = block_sum2(ppq, 0.0, red).x;
+            for (int i = threadIdx.x; i < n; i += NT) ppq += p[i] * q[i];
+            const double pq = block_sum2<NT>(ppq, 0.0, red).x;
             if (!(pq > 0.0)) break;  // breakdown: the true residual decides below
             const double alpha = rz / pq;
             double prr = 0.0, prz = 0.0;
-            for (int i = threadIdx.x; i < n; i += kThreads) {
+            for (int i = threadIdx.x; i < n; i += NT) {
                 x[i] += alpha * p[i];
                 const double ri = r[i] - alpha * q[i];
                 r[i] = ri;
                 prr += ri * ri;
                 prz += ri * ri / a.diag[i];
             }
-            t = block_sum2(prr, prz, red);
+            t = block_sum2<NT>(prr, prz, red);
             rr = t.x;
             const double beta = t.y / rz;
             rz = t.y;
-            for (int i = threadIdx.x; i < n; i += kThreads) p[i] = r[i] / a.diag[i] + beta * p[i];
+            for (int i = threadIdx.x; i < n; i += NT) p[i] = r[i] / a.diag[i] + beta * p[i];
             __syncthreads();
             ++it;
         }
         // the true residual, and a restart from it unless the solve is done
-        spmv(a, x, q, bad);
+        spmv<NT>(a, x, q, bad);
         __syncthreads();
         pr = 0.0;
         pz = 0.0;
-        for (int i = threadIdx.x; i < n; i += kThreads) {
+        for (int i = threadIdx.x; i < n; i += NT) {
             const double ri = rhs(a, i, s, d) - q[i];
             r[i] = ri;
             p[i] = ri / a.diag[i];
             pr += ri * ri;
             pz += ri * ri / a.diag[i];
         }
-        t = block_sum2(pr, pz, red);
+        t = block_sum2<NT>(pr, pz, red);
         rr = t.x;
         rz = t.y;
         if (rr <= goal || it >= a.max_iter) break;
@@ -139,13 +141,13 @@ __device__ void solve_job(const GArgs &a, int64_t j, double *r, double *p, doubl
     __syncthreads();
     const double xs = x[s];
     __syncthreads();
-    for (int i = threadIdx.x; i < n; i += kThreads) x[i] -= xs;
+    for (int i = threadIdx.x; i < n; i += NT) x[i] -= xs;
     __syncthreads();
     if (a.cur) {
         // graph_node_currents: the largest branch current into and out of any node, then each node's inflow and
         // outflow in adjacency order, leaving out branches under 1e-8 of the largest
         double mi = -INFINITY, mo = -INFINITY;
-        for (int c = threadIdx.x; c < n; c += kThreads) {
+        for (int c = threadIdx.x; c < n; c += NT) {
             const double vc = x[c];
             for (int64_t e = a.ptr[c]; e < a.ptr[c + 1]; ++e) {
                 const int k = a.adj[e];
@@ -158,9 +160,9 @@ __device__ void solve_job(const GArgs &a, int64_t j, double *r, double *p, doubl
                 }
             }
         }
-        const double2 m = block_max2(mi, mo, red);
+        const double2 m = block_max2<NT>(mi, mo, red);
         double *cj = a.cur + static_cast<size_t>(j) * n;
-        for (int c = threadIdx.x; c < n; c += kThreads) {
+        for (int c = threadIdx.x; c < n; c += NT) {
             const double vc = x[c];
             double in = 0.0, out = 0.0;
             for (int64_t e = a.ptr[c]; e < a.ptr[c + 1]; ++e) {
@@ -177,13 +179,14 @@ __device__ void solve_job(const GArgs &a, int64_t j, double *r, double *p, doubl
         }
     }
     // `bad` is per thread: any thread that met an out-of-range column fails the job
-    const double anybad = block_sum2(bad ? 1.0 : 0.0, 0.0, red).x;
+    const double anybad = block_sum2<NT>(bad ? 1.0 : 0.0, 0.0, red).x;
     if (threadIdx.x == 0)
         a.jstat[j] = JobStat{anybad > 0 ? -1 : it, (anybad == 0 && resid <= a.accept) ? 1 : 0, resid};
 }
 
-__global__ void __launch_bounds__(kThreads) k_graph_pairs(GArgs a) {
-    __shared__ double2 red[kWarps];
+template <int NT>
+__global__ void __launch_bounds__(NT) k_graph_pairs(GArgs a) {
+    __shared__ double2 red[NT / 32];
     __shared__ long long s_job;
     double *r = a.scratch + static_cast<size_t>(blockIdx.x) * 3 * a.n;
     double *p = r + a.n, *q = p + a.n;
@@ -194,7 +197,7 @@ __global__ void __launch_bounds__(kThreads) k_graph_pairs(GArgs a) {
         __syncthreads();
         const long long j = s_job;
         if (j >= a.n_jobs) return;
-        solve_job(a, j, r, p, q, red);
+        solve_job<NT>(a, j, r, p, q, red);
     }
 }
 
@@ -205,7 +208,7 @@ struct GraphPlan {
 
 GraphPlan plan(int64_t n, int64_t n_jobs, const lsb_graph_params *p) {
     GraphPlan g{};
-    const int64_t cap = p->max_ctas > 0 ? p->max_ctas : 4LL * device_sms();
+    const int64_t cap = p->max_ctas > 0 ? p->max_ctas : static_cast<int64_t>(ctas_per_sm(threads_for(n))) * device_sms();
     const int64_t memcap = std::max<int64_t>(1, static_cast<int64_t>(kScratchCap / (24.0 * static_cast<double>(n))));
     g.ctas = std::max<int64_t>(1, std::min({n_jobs, cap, memcap}));
     g.off_stats = kAlign;  // the job counter sits at offset 0
@@ -278,7 +281,10 @@ int lsb_graph_pairs(int64_t n, const int64_t *ptr, const int32_t *adj, const dou
     a.scratch = reinterpret_cast<double *>(ws + g.off_scratch);
     cudaError_t e = cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), st);
     if (e == cudaSuccess) {
-        k_graph_pairs<<<static_cast<unsigned>(g.ctas), kThreads, 0, st>>>(a);
+        if (threads_for(n) == 512)
+            k_graph_pairs<512><<<static_cast<unsigned>(g.ctas), 512, 0, st>>>(a);
+        else
+            k_graph_pairs<256><<<static_cast<unsigned>(g.ctas), 256, 0, st>>>(a);
         e = cudaGetLastError();
     }
     if (e != cudaSuccess) {

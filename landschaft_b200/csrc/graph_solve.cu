@@ -40,9 +40,10 @@ struct SArgs {
 
 // y = A v on the unknowns (rows of direct grounds are 0; v is 0 there).  Entries whose column is out of range are
 // skipped and counted in `bad`.
+template <int NT>
 __device__ __forceinline__ void spmv(const SArgs &a, const double *dg, const uint8_t *mask, const double *v,
                                      double *y, int &bad) {
-    for (int i = threadIdx.x; i < a.n; i += kThreads) {
+    for (int i = threadIdx.x; i < a.n; i += NT) {
         double s = 0.0;
         if (!mask[i]) {
             s = dg[i] * v[i];
@@ -59,13 +60,14 @@ __device__ __forceinline__ void spmv(const SArgs &a, const double *dg, const uin
     }
 }
 
+template <int NT>
 __device__ void solve_problem(const SArgs &a, int64_t j, double *scr, double2 *red) {
     const int n = a.n;
     double *x = a.volt + static_cast<size_t>(j) * n;
     double *r = scr, *p = r + n, *q = p + n, *b = q + n, *dg = b + n, *fin = dg + n;
     uint8_t *mask = reinterpret_cast<uint8_t *>(fin + n);
     int bad = 0;
-    for (int i = threadIdx.x; i < n; i += kThreads) {
+    for (int i = threadIdx.x; i < n; i += NT) {
         x[i] = 0.0;
         b[i] = 0.0;
         dg[i] = a.diag[i];
@@ -74,14 +76,14 @@ __device__ void solve_problem(const SArgs &a, int64_t j, double *scr, double2 *r
     }
     __syncthreads();
     // the job's lists (nodes unique within each list)
-    for (int64_t e = a.d_ptr[j] + threadIdx.x; e < a.d_ptr[j + 1]; e += kThreads) {
+    for (int64_t e = a.d_ptr[j] + threadIdx.x; e < a.d_ptr[j + 1]; e += NT) {
         const int v = a.d_node[e];
         if (v < 0 || v >= n)
             bad = 1;
         else
             mask[v] = 1;
     }
-    for (int64_t e = a.f_ptr[j] + threadIdx.x; e < a.f_ptr[j + 1]; e += kThreads) {
+    for (int64_t e = a.f_ptr[j] + threadIdx.x; e < a.f_ptr[j + 1]; e += NT) {
         const int v = a.f_node[e];
         if (v < 0 || v >= n) {
             bad = 1;
@@ -90,7 +92,7 @@ __device__ void solve_problem(const SArgs &a, int64_t j, double *scr, double2 *r
             dg[v] = a.diag[v] + a.f_val[e];
         }
     }
-    for (int64_t e = a.s_ptr[j] + threadIdx.x; e < a.s_ptr[j + 1]; e += kThreads) {
+    for (int64_t e = a.s_ptr[j] + threadIdx.x; e < a.s_ptr[j + 1]; e += NT) {
         const int v = a.s_node[e];
         if (v < 0 || v >= n)
             bad = 1;
@@ -100,7 +102,7 @@ __device__ void solve_problem(const SArgs &a, int64_t j, double *scr, double2 *r
     __syncthreads();
     // b on the unknowns only (a direct ground is not an unknown); r = b, p = D^-1 r
     double pr = 0.0, pz = 0.0;
-    for (int i = threadIdx.x; i < n; i += kThreads) {
+    for (int i = threadIdx.x; i < n; i += NT) {
         if (mask[i]) b[i] = 0.0;
         const double bi = b[i];
         r[i] = bi;
@@ -108,7 +110,7 @@ __device__ void solve_problem(const SArgs &a, int64_t j, double *scr, double2 *r
         pr += bi * bi;
         pz += bi * bi / dg[i];
     }
-    double2 t = block_sum2(pr, pz, red);
+    double2 t = block_sum2<NT>(pr, pz, red);
     const double bb = t.x;
     double rr = t.x, rz = t.y;
     const double goal = a.tol * a.tol * bb;
@@ -116,42 +118,42 @@ __device__ void solve_problem(const SArgs &a, int64_t j, double *scr, double2 *r
     int it = 0, stall = 0;
     for (int cycle = 0; cycle < kMaxRestarts; ++cycle) {
         while (it < a.max_iter && rr > goal) {
-            spmv(a, dg, mask, p, q, bad);
+            spmv<NT>(a, dg, mask, p, q, bad);
             __syncthreads();
             double ppq = 0.0;
-            for (int i = threadIdx.x; i < n; i += kThreads) ppq += p[i] * q[i];
-            const double pq = block_sum2(ppq, 0.0, red).x;
+            for (int i = threadIdx.x; i < n; i += NT) ppq += p[i] * q[i];
+            const double pq = block_sum2<NT>(ppq, 0.0, red).x;
             if (!(pq > 0.0)) break;  // breakdown: the true residual decides below
             const double alpha = rz / pq;
             double prr = 0.0, prz = 0.0;
-            for (int i = threadIdx.x; i < n; i += kThreads) {
+            for (int i = threadIdx.x; i < n; i += NT) {
                 x[i] += alpha * p[i];
                 const double ri = r[i] - alpha * q[i];
                 r[i] = ri;
                 prr += ri * ri;
                 prz += ri * ri / dg[i];
             }
-            t = block_sum2(prr, prz, red);
+            t = block_sum2<NT>(prr, prz, red);
             rr = t.x;
             const double beta = t.y / rz;
             rz = t.y;
-            for (int i = threadIdx.x; i < n; i += kThreads) p[i] = r[i] / dg[i] + beta * p[i];
+            for (int i = threadIdx.x; i < n; i += NT) p[i] = r[i] / dg[i] + beta * p[i];
             __syncthreads();
             ++it;
         }
         // the true residual, and a restart from it unless the solve is done
-        spmv(a, dg, mask, x, q, bad);
+        spmv<NT>(a, dg, mask, x, q, bad);
         __syncthreads();
         pr = 0.0;
         pz = 0.0;
-        for (int i = threadIdx.x; i < n; i += kThreads) {
+        for (int i = threadIdx.x; i < n; i += NT) {
             const double ri = mask[i] ? 0.0 : b[i] - q[i];
             r[i] = ri;
             p[i] = ri / dg[i];
             pr += ri * ri;
             pz += ri * ri / dg[i];
         }
-        t = block_sum2(pr, pz, red);
+        t = block_sum2<NT>(pr, pz, red);
         rr = t.x;
         rz = t.y;
         if (rr <= goal || it >= a.max_iter) break;
@@ -169,7 +171,7 @@ __device__ void solve_problem(const SArgs &a, int64_t j, double *scr, double2 *r
         // node's inflow and outflow in adjacency order (branches under 1e-8 of the largest left out), plus the
         // current through its finite ground
         double mi = -INFINITY, mo = -INFINITY;
-        for (int c = threadIdx.x; c < n; c += kThreads) {
+        for (int c = threadIdx.x; c < n; c += NT) {
             const double vc = x[c];
             for (int64_t e = a.ptr[c]; e < a.ptr[c + 1]; ++e) {
                 const int k = a.adj[e];
@@ -182,9 +184,9 @@ __device__ void solve_problem(const SArgs &a, int64_t j, double *scr, double2 *r
                 }
             }
         }
-        const double2 m = block_max2(mi, mo, red);
+        const double2 m = block_max2<NT>(mi, mo, red);
         double *cj = a.cur + static_cast<size_t>(j) * n;
-        for (int c = threadIdx.x; c < n; c += kThreads) {
+        for (int c = threadIdx.x; c < n; c += NT) {
             const double vc = x[c];
             double in = 0.0, out = 0.0;
             for (int64_t e = a.ptr[c]; e < a.ptr[c + 1]; ++e) {
@@ -206,13 +208,14 @@ __device__ void solve_problem(const SArgs &a, int64_t j, double *scr, double2 *r
         }
     }
     // `bad` is per thread: any thread that met a node out of range fails the job
-    const double anybad = block_sum2(bad ? 1.0 : 0.0, 0.0, red).x;
+    const double anybad = block_sum2<NT>(bad ? 1.0 : 0.0, 0.0, red).x;
     if (threadIdx.x == 0)
         a.jstat[j] = JobStat{anybad > 0 ? -1 : it, (anybad == 0 && resid <= a.accept) ? 1 : 0, resid};
 }
 
-__global__ void __launch_bounds__(kThreads) k_graph_solve(SArgs a) {
-    __shared__ double2 red[kWarps];
+template <int NT>
+__global__ void __launch_bounds__(NT) k_graph_solve(SArgs a) {
+    __shared__ double2 red[NT / 32];
     __shared__ long long s_job;
     double *scr = a.scratch + static_cast<size_t>(blockIdx.x) * kPerNode * a.n;
     // each pass takes a new job index; the counter only grows, so the loop ends after n_jobs + gridDim.x passes
@@ -222,7 +225,7 @@ __global__ void __launch_bounds__(kThreads) k_graph_solve(SArgs a) {
         __syncthreads();
         const long long j = s_job;
         if (j >= a.n_jobs) return;
-        solve_problem(a, j, scr, red);
+        solve_problem<NT>(a, j, scr, red);
     }
 }
 
@@ -233,7 +236,7 @@ struct SolvePlan {
 
 SolvePlan plan(int64_t n, int64_t n_jobs, const lsb_graph_params *p) {
     SolvePlan g{};
-    const int64_t cap = p->max_ctas > 0 ? p->max_ctas : 4LL * device_sms();
+    const int64_t cap = p->max_ctas > 0 ? p->max_ctas : static_cast<int64_t>(ctas_per_sm(threads_for(n))) * device_sms();
     const int64_t memcap =
         std::max<int64_t>(1, static_cast<int64_t>(kScratchCap / (8.0 * kPerNode * static_cast<double>(n))));
     g.ctas = std::max<int64_t>(1, std::min({n_jobs, cap, memcap}));
@@ -302,7 +305,10 @@ int lsb_graph_solve(int64_t n, const int64_t *ptr, const int32_t *adj, const dou
     a.scratch = reinterpret_cast<double *>(ws + g.off_scratch);
     cudaError_t e = cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), st);
     if (e == cudaSuccess) {
-        k_graph_solve<<<static_cast<unsigned>(g.ctas), kThreads, 0, st>>>(a);
+        if (threads_for(n) == 512)
+            k_graph_solve<512><<<static_cast<unsigned>(g.ctas), 512, 0, st>>>(a);
+        else
+            k_graph_solve<256><<<static_cast<unsigned>(g.ctas), 256, 0, st>>>(a);
         e = cudaGetLastError();
     }
     if (e != cudaSuccess) {

@@ -239,3 +239,24 @@ def test_node_sums_and_conflicts_match_the_oracle(policy):
     gnd = np.where(rng.random(graph.n_nodes) < 0.3, rng.choice([0.5, 2.0, np.inf], graph.n_nodes), 0.0)
     for a, b in zip(cs.resolve_conflicts(src, gnd, policy), O.resolve(list(src), list(gnd), policy)):
         np.testing.assert_array_equal(a, np.array(b))
+
+
+def test_pair_solver_routing():
+    g = np.exp(np.random.default_rng(8).normal(size=(9, 7)))
+    g[2, 3] = 0
+    plain = cs.raster_graph(g, None, False, False)
+    assert cs.raster_route(plain) and not plain.merged
+    poly = np.zeros(g.shape, dtype=np.int64)
+    poly[4:6, 1:3] = 1
+    assert cs.raster_graph(g, poly, False, False).merged  # four cells in one node
+    lone = np.zeros(g.shape, dtype=np.int64)
+    lone[0, 0] = 5
+    assert not cs.raster_graph(g, lone, False, False).merged  # a one-cell region is a plain node
+    assert not cs.raster_route(cs.raster_graph(g, None, True, False))  # resistor-series weights
+    pts = np.array([0, 5])
+    ex = np.zeros((2, 2), dtype=bool)
+    with pytest.raises(ValueError, match="pair_solver"):
+        cs.raster_pairwise(plain, g, pts, ex, cs.PairOptions(), pair_solver="direct")
+    with pytest.raises(ValueError, match="plain grid"):
+        cs.raster_pairwise(cs.raster_graph(g, poly, False, False), g, pts, ex, cs.PairOptions(),
+                           pair_solver="raster")

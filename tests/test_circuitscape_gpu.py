@@ -28,9 +28,10 @@ def in_cs(monkeypatch):
     monkeypatch.chdir(CS)
 
 
+@pytest.mark.parametrize("pair_solver", ["auto", "graph"])
 @pytest.mark.parametrize("name", POINT_CASES + REGION_CASES)
-def test_pairwise_matches_circuitscape(name, in_cs):
-    r = cs.circuitscape_ini(ini_path(name))
+def test_pairwise_matches_circuitscape(name, pair_solver, in_cs):
+    r = cs.circuitscape_ini(ini_path(name), pair_solver=pair_solver)
     check_against_golden(name, r.resistances, r.cum_current, r.max_current, r.maps)
     assert r.stats.failures == 0 and r.stats.jobs > 0
 
@@ -67,8 +68,9 @@ def oracle_pairwise(g, poly, pm, avg, four, opts, excluded_ids=frozenset()):
     return R, cum, mx, maps
 
 
+@pytest.mark.parametrize("pair_solver", ["auto", "graph"])
 @pytest.mark.parametrize("seed", range(6))
-def test_random_rasters_match_the_oracle(seed):
+def test_random_rasters_match_the_oracle(seed, pair_solver):
     rng = np.random.default_rng(100 + seed)
     ny, nx = (int(v) for v in rng.integers(8, 40, 2))
     g, poly = random_case(rng, ny, nx, seed % 2 == 0)
@@ -80,7 +82,7 @@ def test_random_rasters_match_the_oracle(seed):
                  set_focal_node_currents_to_zero=seed == 3, set_null_currents_to_nodata=seed == 4,
                  set_null_voltages_to_nodata=seed == 4, log_transform_maps=seed == 5)
     r = cs.circuitscape_pairwise(g, pm, habitat_is_resistance=False, polygons=poly, four_neighbors=four,
-                                 avg_resistances=avg, **flags)
+                                 avg_resistances=avg, pair_solver=pair_solver, **flags)
     opts = {"volt_maps": True, "cur_maps": True, "cum": True, "max": True, "focal_zero": seed == 3,
             "null_currents": seed == 4, "null_voltages": seed == 4, "log_transform": seed == 5}
     R, cum, mx, maps = oracle_pairwise(g, poly, pm, avg, four, opts)
@@ -111,14 +113,17 @@ def test_shortcut_matches_full_solves_and_excluded_pairs():
     assert ex.resistances[1, 2] == -1 and ex.resistances[2, 1] == -1
 
 
-def test_larger_raster_matches_the_oracle():
+@pytest.mark.parametrize("pair_solver", ["raster", "graph"])
+def test_larger_raster_matches_the_oracle(pair_solver):
+    # over 8,192 nodes: the kernel runs 512 threads per CTA
     rng = np.random.default_rng(11)
-    ny, nx = 96, 80
+    ny, nx = 112, 96
     g = 10 ** rng.uniform(0, 2, size=(ny, nx))
     g[rng.random((ny, nx)) < 0.1] = 0
     pm = np.zeros((ny, nx))
     pm.flat[rng.choice(ny * nx, size=5, replace=False)] = np.arange(1, 6)
-    r = cs.circuitscape_pairwise(g, pm, habitat_is_resistance=False, cum_map=True, max_map=True)
+    r = cs.circuitscape_pairwise(g, pm, habitat_is_resistance=False, cum_map=True, max_map=True,
+                                 pair_solver=pair_solver)
     R, cum, mx, _ = oracle_pairwise(g, None, pm, False, False, {"cum": True, "max": True})
     np.testing.assert_allclose(r.resistances[1:, 1:], R, rtol=1e-9)
     np.testing.assert_allclose(r.cum_current, cum.reshape(ny, nx), rtol=1e-8, atol=1e-10 * np.abs(cum).max())
@@ -309,3 +314,19 @@ def test_graph_solve_closed_form():
     np.testing.assert_allclose(c[0], np.ones(4), rtol=1e-12)  # the finite ground's current counts at node 3
     np.testing.assert_allclose(v[1], [1 / 2 + 1 / 0.5 + 1 / 4, 1 / 0.5 + 1 / 4, 1 / 4, 0.0], rtol=1e-12, atol=1e-15)
     np.testing.assert_allclose(c[1], np.ones(4), rtol=1e-12)
+
+
+def test_large_advanced_matches_the_oracle():
+    # over 8,192 nodes (512 threads per CTA), finite and direct grounds, several sources
+    rng = np.random.default_rng(61)
+    ny, nx = 104, 96
+    g = 10 ** rng.uniform(0, 2, size=(ny, nx))
+    g[rng.random((ny, nx)) < 0.05] = 0
+    src = np.zeros((ny, nx))
+    src.flat[rng.choice(ny * nx, 5, replace=False)] = rng.uniform(0.5, 2.0, 5)
+    gr = np.zeros((ny, nx))
+    gr.flat[rng.choice(ny * nx, 3, replace=False)] = [np.inf, 0.7, 3.0]
+    r = cs._advanced(g, None, src, gr, False, False, "keepall", False, False, cs.multi_advanced)
+    want = cs._advanced(g, None, src, gr, False, False, "keepall", False, False, O.multi_advanced)
+    for ours, ref in ((r.voltage, want.voltage), (r.current, want.current)):
+        np.testing.assert_allclose(ours, ref, rtol=1e-9, atol=1e-11 * np.abs(ref).max())
