@@ -671,11 +671,21 @@ def raster_pairwise(graph: RasterGraph, gmap: np.ndarray, points: np.ndarray, ex
         in_k = cell_comp == k
         cells_k = np.flatnonzero(in_k)
         node_q = np.searchsorted(members, graph.nodemap[cells_k])
+        # only the cum / max maps, one focal point per node: each job adds its current map once, so the maps follow
+        # from the jobs' currents at once (the sum runs over the jobs in order, as the per-pair additions do)
+        summed = (o.maps() and not (o.volt_maps or o.cur_maps or o.focal_zero or o.log_transform or o.null_currents)
+                  and all(len(positions[v]) == 1 for v in csub))
+        if summed:
+            if o.cum:
+                cum[cells_k] += np.add.reduce(cur, axis=0)[node_q]
+            if o.max:
+                np.maximum(mx, 0.0, out=mx)
+                mx[cells_k] = np.maximum(mx[cells_k], cur.max(axis=0)[node_q])
         for jn, (s, d) in enumerate(jobs):
             vcol = volt[jn]
             resistance = vcol[mindex[d]] - vcol[mindex[s]]
             vmap = cmap = None
-            if o.maps():
+            if o.maps() and not summed:
                 if o.volt_maps:
                     vmap = np.zeros(ncell)
                     vmap[cells_k] = vcol[node_q]
@@ -703,7 +713,7 @@ def raster_pairwise(graph: RasterGraph, gmap: np.ndarray, points: np.ndarray, ex
                                 continue
                             voltmatrix[i, cj] = 1 - vcol[mindex[v]] / resistance
                         continue
-                    if not o.maps():
+                    if not o.maps() or summed:
                         continue
                     if o.cum:
                         cum += cmap

@@ -260,3 +260,31 @@ def test_pair_solver_routing():
     with pytest.raises(ValueError, match="plain grid"):
         cs.raster_pairwise(cs.raster_graph(g, poly, False, False), g, pts, ex, cs.PairOptions(),
                            pair_solver="raster")
+
+
+def test_summed_maps_equal_the_per_pair_maps(monkeypatch):
+    # the cum / max maps from the jobs' currents at once are bitwise those of the per-pair additions (the solve is
+    # replaced by a deterministic fake, so this runs without a GPU)
+    def fake(graph, members, ground, src, dst, want_currents, params, stats, dev):
+        r = np.random.default_rng(int(src.sum() * 7 + dst.sum()))
+        v = r.normal(size=(len(src), len(members)))
+        c = np.abs(r.normal(size=(len(src), len(members))))
+        return v, (c if want_currents else None)
+
+    monkeypatch.setattr(cs, "_solve_component", fake)
+    rng = np.random.default_rng(0)
+    for trial in range(12):
+        ny, nx = (int(v) for v in rng.integers(5, 30, 2))
+        g = np.exp(rng.normal(size=(ny, nx)))
+        g[rng.random((ny, nx)) < 0.3] = 0
+        graph = cs.raster_graph(g, None, False, False)
+        pts = rng.permutation(np.unique(graph.nodemap[graph.nodemap >= 0])[:7])
+        ex = np.zeros((len(pts), len(pts)), dtype=bool)
+        if trial % 3 == 0:
+            ex[0, 1] = ex[1, 0] = True
+        a = cs.raster_pairwise(graph, g, pts, ex, cs.PairOptions(cum=True, max=True), device="cpu",
+                               pair_solver="graph")
+        b = cs.raster_pairwise(graph, g, pts, ex, cs.PairOptions(cum=True, max=True, cur_maps=True),
+                               lambda *x: None, device="cpu", pair_solver="graph")
+        for x, y in zip(a, b):
+            np.testing.assert_array_equal(x, y)
