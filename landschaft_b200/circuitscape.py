@@ -537,11 +537,13 @@ def raster_route(graph: RasterGraph) -> bool:
 
 
 def _solve_component_rasters(graph: RasterGraph, gmap: np.ndarray, members: np.ndarray, src: np.ndarray,
-                             dst: np.ndarray, want_currents: bool, tol: float, stats: GraphSolveStats, device):
+                             dst: np.ndarray, want_currents: bool, tol: float, stats: GraphSolveStats, device,
+                             focal: np.ndarray | None = None):
     """The jobs of one component on the raster solver (lsb_rasters: FP32 CG with a multigrid preconditioner inside
     FP64 refinement): job j is the raster with a unit source at dst[j]'s cell and a direct ground at src[j]'s, whose
     voltages are the pair's voltages relative to its source and whose node currents are the pair's.  Same contract
-    as _solve_component."""
+    as _solve_component; with ``focal`` (member indices) it returns instead (the voltages at those members, jobs x
+    focal; the currents summed over the jobs; their maximum over the jobs), reduced on the device."""
     import torch
 
     from . import raster as R
@@ -552,8 +554,14 @@ def _solve_component_rasters(graph: RasterGraph, gmap: np.ndarray, members: np.n
     node_cell[graph.nodemap[on]] = on
     mcell = torch.from_numpy(node_cell[members]).to(device)
     nj = len(src)
-    volt = np.empty((nj, len(members)))
-    cur = np.empty((nj, len(members))) if want_currents else None
+    if focal is not None:
+        fcell = torch.from_numpy(node_cell[members[focal]]).to(device)
+        volt = np.empty((nj, len(focal)))
+        c_sum = torch.zeros(len(members), dtype=torch.float64, device=device)
+        c_max = torch.full((len(members),), -np.inf, dtype=torch.float64, device=device)
+    else:
+        volt = np.empty((nj, len(members)))
+        cur = np.empty((nj, len(members))) if want_currents else None
     p = R.raster_params(four_neighbors=graph.four_neighbors, tol=tol)
     g_dev = torch.from_numpy(np.ascontiguousarray(gmap, dtype=np.float64).ravel()).to(device)
     per = max(1, min(nj, (1 << 31) // (40 * ncell)))  # inputs and outputs of a batch within 2 GiB
@@ -566,13 +574,21 @@ def _solve_component_rasters(graph: RasterGraph, gmap: np.ndarray, members: np.n
         S[base + torch.from_numpy(node_cell[dst[b0:b1]]).to(device)] = 1.0
         GR[base + torch.from_numpy(node_cell[src[b0:b1]]).to(device)] = np.inf
         c, v, st = R.run_rasters(g_dev.repeat(nb), S, GR, [(ny, nx)] * nb, p)
-        volt[b0:b1] = v.view(nb, ncell)[:, mcell].cpu().numpy()
-        if want_currents:
-            cur[b0:b1] = c.view(nb, ncell)[:, mcell].cpu().numpy()
+        if focal is not None:
+            volt[b0:b1] = v.view(nb, ncell)[:, fcell].cpu().numpy()
+            cm = c.view(nb, ncell)[:, mcell]
+            c_sum += cm.sum(dim=0)
+            c_max = torch.maximum(c_max, cm.max(dim=0).values)
+        else:
+            volt[b0:b1] = v.view(nb, ncell)[:, mcell].cpu().numpy()
+            if want_currents:
+                cur[b0:b1] = c.view(nb, ncell)[:, mcell].cpu().numpy()
         mean = st.iters_total / max(st.n_solved, 1)
         stats.iters_mean = (stats.iters_mean * stats.jobs + mean * nb) / (stats.jobs + nb)
         stats.jobs += nb
         stats.iters_max = max(stats.iters_max, int(st.iters_max))
+    if focal is not None:
+        return volt, c_sum.cpu().numpy(), c_max.cpu().numpy()
     return volt, cur
 
 
@@ -662,25 +678,35 @@ def raster_pairwise(graph: RasterGraph, gmap: np.ndarray, points: np.ndarray, ex
         ground = int(members[-1])
         src = np.array([j[0] for j in jobs], dtype=np.int64)
         dst = np.array([j[1] for j in jobs], dtype=np.int64)
-        if on_rasters:
+        # only the cum / max maps, one focal point per node: each job adds its current map once, so the maps follow
+        # from the jobs' currents at once (on the host the sum runs over the jobs in order, as the per-pair additions
+        # do; the raster route reduces on the device)
+        summed = (o.maps() and not (o.volt_maps or o.cur_maps or o.focal_zero or o.log_transform or o.null_currents)
+                  and all(len(positions[v]) == 1 for v in csub))
+        mindex = {int(v): q for q, v in enumerate(members)}
+        c_sum = c_max = None
+        if on_rasters and summed:
+            fq = np.array([mindex[v] for v in csub], dtype=np.int64)
+            volt, c_sum, c_max = _solve_component_rasters(graph, gmap, members, src, dst, True, min(tol, 1e-12),
+                                                          stats, dev, focal=fq)
+            mindex = {v: i for i, v in enumerate(csub)}  # the loop below reads the focal voltages only
+            cur = None
+        elif on_rasters:
             volt, cur = _solve_component_rasters(graph, gmap, members, src, dst, o.maps(), min(tol, 1e-12), stats,
                                                  dev)
         else:
             volt, cur = _solve_component(graph, members, ground, src, dst, o.maps(), params, stats, dev)
-        mindex = {int(v): q for q, v in enumerate(members)}
         in_k = cell_comp == k
         cells_k = np.flatnonzero(in_k)
         node_q = np.searchsorted(members, graph.nodemap[cells_k])
-        # only the cum / max maps, one focal point per node: each job adds its current map once, so the maps follow
-        # from the jobs' currents at once (the sum runs over the jobs in order, as the per-pair additions do)
-        summed = (o.maps() and not (o.volt_maps or o.cur_maps or o.focal_zero or o.log_transform or o.null_currents)
-                  and all(len(positions[v]) == 1 for v in csub))
         if summed:
+            if c_sum is None:
+                c_sum, c_max = np.add.reduce(cur, axis=0), cur.max(axis=0)
             if o.cum:
-                cum[cells_k] += np.add.reduce(cur, axis=0)[node_q]
+                cum[cells_k] += c_sum[node_q]
             if o.max:
                 np.maximum(mx, 0.0, out=mx)
-                mx[cells_k] = np.maximum(mx[cells_k], cur.max(axis=0)[node_q])
+                mx[cells_k] = np.maximum(mx[cells_k], c_max[node_q])
         for jn, (s, d) in enumerate(jobs):
             vcol = volt[jn]
             resistance = vcol[mindex[d]] - vcol[mindex[s]]
