@@ -364,8 +364,11 @@ def bench_pairwise(args, rank, world, local, d):
                 "data": "synthetic (seeded Gaussian random field, 24 random focal points)",
                 "config": {"workload": "pairwise_256", "nodes": n, "pairs": nj, "neighbours": 8,
                            "l2": "flushed between timed steps (256 MiB write)", "tol": 1e-12},
-                "e2e": {"value": world * nj / TE, "unit": "pairs/s", "h2d_bytes_per_step": int(2 * 8 * g.size),
-                        "d2h_bytes_per_step": int(nj * 2 * 8 * n), "includes": "host graph build and map assembly"},
+                "e2e": {"value": world * nj / TE, "unit": "pairs/s",
+                        "h2d_bytes_per_step": int(8 * g.size + 2 * 8 * nj),
+                        "d2h_bytes_per_step": int(8 * nj * len(nodes) + 2 * 8 * n),
+                        "includes": "host graph build; the conductance raster and the pairs' cells in, the focal "
+                                    "voltages and the summed and largest currents out; the cum map on the host"},
                 "solver": "lsb_rasters (FP32 CG, multigrid, FP64 refinement to 1e-12)",
                 "cg_iterations": {"mean": rst.iters_total / max(rst.n_solved, 1), "max": rst.iters_max},
                 "graph_kernel": {"value": world * nj / t_graph, "unit": "pairs/s", "kernel": "lsb_graph_pairs",
