@@ -54,6 +54,8 @@ def _grid(values, name: str):
         if nodata is not None and not np.isnan(nodata):
             v[v == nodata] = np.nan
         like = da
+    elif isinstance(values, np.ndarray) and not isinstance(values, np.ma.MaskedArray):
+        v = np.asarray(values, dtype=np.float64)  # no copy for float64: the callers only read it
     else:
         v = np.array(np.ma.filled(np.ma.asarray(values, dtype=np.float64), np.nan), dtype=np.float64)
     if v.ndim != 2:
@@ -527,8 +529,7 @@ def omniscape(resistance, radius, *, source=None, block_size=1, buffer=0, source
     r, like = _grid(resistance, "resistance")
     if dtype is np.float32:
         r = r.astype(np.float32).astype(np.float64)
-    finite = r[~np.isnan(r)]
-    if finite.size and finite.min() <= 0:
+    if np.any(r <= 0):  # NaN (NoData) compares false
         raise ValueError("resistance (or conductance) values must be > 0")
     radius = _to_int(radius, "radius")
     buffer = _to_int(buffer, "buffer")
@@ -547,15 +548,13 @@ def omniscape(resistance, radius, *, source=None, block_size=1, buffer=0, source
             raise ValueError("the source raster must have the resistance's shape")
         if dtype is np.float32:
             s = s.astype(np.float32).astype(np.float64)
-        s = np.where(np.isnan(s), 0.0, s)
-        s = np.where(s < source_threshold, 0.0, s)
+        s = np.where(np.isnan(s) | (s < source_threshold), 0.0, s)
     s = np.ascontiguousarray(s, dtype=np.float64)
     if reclass_table is not None:
         r = reclassify(r, reclass_table)
         if dtype is np.float32:
             r = r.astype(np.float32).astype(np.float64)
-        finite = r[~np.isnan(r)]
-        if finite.size and finite.min() <= 0:
+        if np.any(r <= 0):
             raise ValueError("the reclassified resistance must be > 0")
     r = np.ascontiguousarray(r)
 
