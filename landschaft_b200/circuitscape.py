@@ -371,9 +371,13 @@ def raster_graph(gmap: np.ndarray, polymap: np.ndarray | None, avg_resistances: 
             W.append(w)
             order.append((rank * 4 + d) * 2 + first)
     A, B, W, order = (np.concatenate(x) if x else np.zeros(0) for x in (A, B, W, order))
-    o = np.argsort(order, kind="stable")
+    # back to the order met (the emission keys are distinct integers below 8 x cells: a counting scatter), then a
+    # stable sort by (row, column): duplicates keep the order met
+    slot = np.full(len(cm) * 8, -1, dtype=np.int64)  # keys (rank x 4 + direction) x 2 + orientation
+    slot[order.astype(np.int64)] = np.arange(len(order))
+    o = slot[slot >= 0]
     A, B, W = A[o].astype(np.int64), B[o].astype(np.int64), W[o]
-    s = np.lexsort((B, A))  # stable: duplicates keep the order met
+    s = np.argsort(A * max(n_nodes, 1) + B, kind="stable")
     A, B, W = A[s], B[s], W[s]
     if len(A):
         start = np.flatnonzero(np.r_[True, (A[1:] != A[:-1]) | (B[1:] != B[:-1])])
@@ -388,8 +392,7 @@ def raster_graph(gmap: np.ndarray, polymap: np.ndarray | None, avg_resistances: 
     else:
         wsum = W
     ptr = np.zeros(n_nodes + 1, dtype=np.int64)
-    np.add.at(ptr, A + 1, 1)
-    ptr = np.cumsum(ptr)
+    ptr[1:] = np.cumsum(np.bincount(A, minlength=n_nodes))
     degree = np.zeros(n_nodes)
     # the diagonal sums each row's entries in adjacency order
     for k in range(int(np.diff(ptr).max()) if n_nodes and len(A) else 0):
@@ -452,8 +455,8 @@ def component_system(graph: RasterGraph, members: np.ndarray) -> ComponentSystem
     keep = la >= 0
     rowid = np.repeat(np.arange(m), lens)[keep]
     ptr = np.zeros(m + 1, dtype=np.int64)
-    np.add.at(ptr, rowid + 1, 1)
-    return ComponentSystem(members, local, np.cumsum(ptr), la[keep].astype(np.int32), graph.w[idx][keep],
+    ptr[1:] = np.cumsum(np.bincount(rowid, minlength=m))
+    return ComponentSystem(members, local, ptr, la[keep].astype(np.int32), graph.w[idx][keep],
                            graph.degree[members] + K_SHIFT)
 
 
