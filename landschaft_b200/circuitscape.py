@@ -1116,10 +1116,79 @@ def advanced_many(graph: RasterGraph, srcs, gnds, only_nodes, policy: str, *, to
     return out
 
 
-def multi_advanced(g, poly, avg: bool, four: bool, problems, policy: str, *, tol=1e-13, device=None, stats=None):
+def _advanced_rasters(graph: RasterGraph, gmap, srcs, gnds, only_nodes, policy: str, tol: float, device):
+    """advanced_many on the raster solver (lsb_rasters, multigrid), for a plain grid graph and problems on which the
+    conflict policy decides nothing (no node with both a source and a ground): each problem becomes one raster with
+    its sources and grounds on the components Circuitscape solves (a nonzero source sum and a nonzero ground sum,
+    the check node's component only when there is one), zero elsewhere; the raster solver then solves exactly those
+    components, with finite grounds on the diagonal and in the node currents.  Returns None when a problem does not
+    qualify."""
+    import torch
+
+    from . import raster as R
+    n = graph.n_nodes
+    for s, g_ in zip(srcs, gnds):
+        if np.any((np.asarray(s) != 0) & (np.asarray(g_) != 0)):
+            return None
+    ny, nx = graph.ny, graph.nx
+    ncell = nx * ny
+    on = np.flatnonzero(graph.nodemap >= 0)
+    node_cell = np.empty(n, dtype=np.int64)
+    node_cell[graph.nodemap[on]] = on
+    out, cells_s, vals_s, cells_g, vals_g = [], [], [], [], []
+    for p, (s, g_) in enumerate(zip(srcs, gnds)):
+        s, g_, _ = resolve_conflicts(np.asarray(s, dtype=np.float64), np.asarray(g_, dtype=np.float64), policy)
+        sum_s = np.bincount(graph.comp, weights=s, minlength=graph.n_comp)  # in node order, as the reference sums
+        direct = np.bincount(graph.comp, weights=(g_ == np.inf).astype(np.float64), minlength=graph.n_comp) > 0
+        sum_g = np.bincount(graph.comp, weights=np.where(g_ == np.inf, 0.0, g_), minlength=graph.n_comp)
+        ok = (sum_s != 0) & (direct | (sum_g != 0))  # a direct ground makes the reference's sum infinite
+        only = int(only_nodes[p])
+        if only == -2:
+            ok[:] = False
+        elif only >= 0:
+            keep = np.zeros_like(ok)
+            keep[graph.comp[only]] = ok[graph.comp[only]]
+            ok = keep
+        node_ok = ok[graph.comp]
+        ns = np.flatnonzero(node_ok & (s != 0))
+        ng = np.flatnonzero(node_ok & (g_ != 0))
+        cells_s.append(node_cell[ns])
+        vals_s.append(s[ns])
+        cells_g.append(node_cell[ng])
+        vals_g.append(g_[ng])
+        out.append({"voltage": np.zeros(n), "current": np.zeros(n), "solved": bool(ok.any()),
+                    "active": np.flatnonzero((s != 0) | (g_ != 0)).astype(np.int32)})
+    g_dev = torch.from_numpy(np.ascontiguousarray(gmap, dtype=np.float64).ravel()).to(device)
+    nc = torch.from_numpy(node_cell).to(device)
+    rp = R.raster_params(four_neighbors=graph.four_neighbors, tol=tol)
+    todo = [p for p in range(len(out)) if out[p]["solved"]]
+    per = max(1, (1 << 31) // (40 * ncell))  # inputs and outputs of a batch within 2 GiB
+    for b0 in range(0, len(todo), per):
+        batch = todo[b0:b0 + per]
+        nb = len(batch)
+        S = torch.zeros(nb * ncell, dtype=torch.float64, device=device)
+        GR = torch.zeros_like(S)
+        for q, p in enumerate(batch):
+            S[torch.from_numpy(q * ncell + cells_s[p]).to(device)] = torch.from_numpy(vals_s[p]).to(device)
+            GR[torch.from_numpy(q * ncell + cells_g[p]).to(device)] = torch.from_numpy(vals_g[p]).to(device)
+        c, v, _ = R.run_rasters(g_dev.repeat(nb), S, GR, [(ny, nx)] * nb, rp)
+        v = v.view(nb, ncell)[:, nc].cpu().numpy()
+        c = c.view(nb, ncell)[:, nc].cpu().numpy()
+        for q, p in enumerate(batch):
+            out[p]["voltage"] = v[q]  # 0 on the components not solved
+            out[p]["current"] = c[q]
+    return out
+
+
+def multi_advanced(g, poly, avg: bool, four: bool, problems, policy: str, *, tol=1e-13, device=None, stats=None,
+                   problem_solver: str = "auto"):
     """The reference's native circuitscape_multi_advanced on the GPU: one graph, many problems given by cells
     (src_cells / src_vals / gnd_cells / gnd_vals, check_cell -1 or a cell whose component alone is solved).
-    Returns (nodemap, results)."""
+    Returns (nodemap, results).  ``problem_solver``: "graph" (lsb_graph_solve, any problem), "raster" (lsb_rasters;
+    plain grid graphs and problems without a node that has both a source and a ground) or "auto" (the raster solver
+    where it applies)."""
+    if problem_solver not in ("auto", "graph", "raster"):
+        raise ValueError('problem_solver must be "auto", "graph" or "raster"')
     graph = raster_graph(g, poly, avg, four)
     srcs, gnds, only = [], [], []
     for q in problems:
@@ -1131,6 +1200,15 @@ def multi_advanced(g, poly, avg: bool, four: bool, problems, policy: str, *, tol
             if o < 0:
                 o = -2
         only.append(o)
+    if problem_solver != "graph" and raster_route(graph):
+        import torch
+        dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        routed = _advanced_rasters(graph, g, srcs, gnds, only, policy, min(tol, 1e-12), dev)
+        if routed is not None:
+            return graph.nodemap.reshape(g.shape), routed
+    if problem_solver == "raster":
+        raise ValueError("the raster problem solver needs a plain grid graph and problems without a node that has "
+                         "both a source and a ground")
     return graph.nodemap.reshape(g.shape), advanced_many(graph, srcs, gnds, only, policy, tol=tol, device=device,
                                                          stats=stats)
 
@@ -1159,7 +1237,8 @@ def circuitscape_advanced(habitat, source, ground, *, habitat_is_resistance: boo
                           ground_is_resistance: bool = True, polygons=None, mask=None, four_neighbors: bool = False,
                           avg_resistances: bool = False, remove_src_or_gnd: str = "keepall",
                           unit_currents: bool = False, direct_grounds: bool = False, reclass: dict | None = None,
-                          n_threads: int = 0, tol: float = 1e-13, device=None) -> CircuitscapeResult:
+                          n_threads: int = 0, tol: float = 1e-13, device=None,
+                          problem_solver: str = "auto") -> CircuitscapeResult:
     """Circuitscape's advanced mode on a node graph (drop-in for ``ls.circuit.circuitscape_advanced``,
     circuitscape.py:406-497): sources and grounds per cell (grounds as resistances unless ``ground_is_resistance``
     is False; 0 / inf = direct), short-circuit polygons, a mask, the conflict policy, unit currents and direct
@@ -1178,7 +1257,7 @@ def circuitscape_advanced(habitat, source, ground, *, habitat_is_resistance: boo
         with np.errstate(divide="ignore"):
             gnd = 1 / gnd
     gnd[nod] = 0.0
-    solver = lambda *a: multi_advanced(*a, tol=tol, device=device)  # noqa: E731
+    solver = lambda *a: multi_advanced(*a, tol=tol, device=device, problem_solver=problem_solver)  # noqa: E731
     return _advanced(g, poly, src, gnd, four_neighbors, avg_resistances, remove_src_or_gnd, unit_currents,
                      direct_grounds, solver)
 
@@ -1354,7 +1433,8 @@ def circuitscape_one_to_all(habitat, points, *, all_to_one: bool = False, habita
                             included_pairs=None, strengths=None, voltage_maps: bool = False,
                             current_maps: bool = False, cum_map: bool = False, max_map: bool = False,
                             set_focal_node_currents_to_zero: bool = False, reclass: dict | None = None,
-                            n_threads: int = 0, tol: float = 1e-13, device=None) -> CircuitscapeResult:
+                            n_threads: int = 0, tol: float = 1e-13, device=None,
+                            problem_solver: str = "auto") -> CircuitscapeResult:
     """Circuitscape's one-to-all (or, with ``all_to_one``, all-to-one) mode on rasters (drop-in for
     ``ls.circuit.circuitscape_one_to_all``, circuitscape.py:854-953).  ``resistances`` has the ids in its first
     column and each point's result in the second (one-to-all: the voltage at the point per unit strength, -1 when
@@ -1380,7 +1460,7 @@ def circuitscape_one_to_all(habitat, points, *, all_to_one: bool = False, habita
 
     opts = {"volt_maps": voltage_maps, "cur_maps": current_maps, "cum": current_maps or cum_map, "max": max_map,
             "focal_zero": set_focal_node_currents_to_zero}
-    solver = lambda *a: multi_advanced(*a, tol=tol, device=device)  # noqa: E731
+    solver = lambda *a: multi_advanced(*a, tol=tol, device=device, problem_solver=problem_solver)  # noqa: E731
     r = _one_to_all(g, poly, points, None if strengths is None else np.asarray(strengths, dtype=np.float64),
                     included_pairs, not all_to_one, four_neighbors, avg_resistances, opts, emit, solver)
     r.maps = maps
@@ -1479,7 +1559,7 @@ def _resolve(name: str, base: Path) -> Path:
 
 
 def circuitscape_ini(path, *, write_outputs: bool = False, tol: float = 1e-13, device=None,
-                     pair_solver: str = "auto", _solver=None) -> CircuitscapeResult:
+                     pair_solver: str = "auto", problem_solver: str = "auto", _solver=None) -> CircuitscapeResult:
     """Run a Circuitscape INI file on rasters (scenarios pairwise, advanced, one-to-all and all-to-one), as the
     reference's ``circuitscape_ini`` does (circuitscape.py:1039-1213); paths are read from the working directory, or
     else next to the INI file.  ``maps`` are keyed as Circuitscape names its files (``voltmap_<id1>_<id2>``,
@@ -1526,7 +1606,8 @@ def circuitscape_ini(path, *, write_outputs: bool = False, tol: float = 1e-13, d
         policy = "keepall"
     if policy not in POLICIES:
         raise ValueError(f"remove_src_or_gnd must be one of {POLICIES}")
-    solver = _solver if _solver is not None else (lambda *a: multi_advanced(*a, tol=tol, device=device))
+    solver = _solver if _solver is not None else (
+        lambda *a: multi_advanced(*a, tol=tol, device=device, problem_solver=problem_solver))
 
     if scenario == "advanced":
         src, gnd = _source_and_ground(need("source_file"), need("ground_file"), meta,

@@ -288,3 +288,15 @@ def test_summed_maps_equal_the_per_pair_maps(monkeypatch):
                                lambda *x: None, device="cpu", pair_solver="graph")
         for x, y in zip(a, b):
             np.testing.assert_array_equal(x, y)
+
+
+def test_problem_solver_option():
+    g = np.exp(np.random.default_rng(9).normal(size=(6, 5)))
+    prob = {"src_cells": np.array([0]), "src_vals": np.array([1.0]), "gnd_cells": np.array([29]),
+            "gnd_vals": np.array([np.inf]), "check_cell": -1}
+    with pytest.raises(ValueError, match="problem_solver"):
+        cs.multi_advanced(g, None, False, False, [prob], "keepall", problem_solver="direct")
+    poly = np.zeros(g.shape, dtype=np.int64)
+    poly[2:4, 1:3] = 1
+    with pytest.raises(ValueError, match="plain grid"):  # merged nodes: not for the raster solver
+        cs.multi_advanced(g, poly, False, False, [prob], "keepall", problem_solver="raster")

@@ -219,15 +219,18 @@ def test_iteration_cap_reports_failure():
 
 # --- advanced, one-to-all and all-to-one (lsb_graph_solve) ---------------------------------------------------------
 
+@pytest.mark.parametrize("problem_solver", ["auto", "graph"])
 @pytest.mark.parametrize("ini", ADVANCED_CASES)
-def test_advanced_matches_circuitscape(ini, in_cs):
-    check_advanced(Path(ini).stem, cs.circuitscape_ini(ini))  # the reference's bar, rtol 1e-9
+def test_advanced_matches_circuitscape(ini, problem_solver, in_cs):
+    # the reference's bar, rtol 1e-9
+    check_advanced(Path(ini).stem, cs.circuitscape_ini(ini, problem_solver=problem_solver))
 
 
+@pytest.mark.parametrize("problem_solver", ["auto", "graph"])
 @pytest.mark.parametrize("ini", ONE_TO_ALL_CASES + ALL_TO_ONE_CASES)
-def test_one_to_all_matches_circuitscape(ini, in_cs):
+def test_one_to_all_matches_circuitscape(ini, problem_solver, in_cs):
     # the reference's bar is 1e-11 for its direct solver; the GPU's iterative solve is held to 1e-9
-    check_one_to_all(Path(ini).stem, cs.circuitscape_ini(ini), rtol=1e-9)
+    check_one_to_all(Path(ini).stem, cs.circuitscape_ini(ini, problem_solver=problem_solver), rtol=1e-9)
 
 
 @pytest.mark.parametrize("policy", cs.POLICIES)
@@ -328,5 +331,53 @@ def test_large_advanced_matches_the_oracle():
     gr.flat[rng.choice(ny * nx, 3, replace=False)] = [np.inf, 0.7, 3.0]
     r = cs._advanced(g, None, src, gr, False, False, "keepall", False, False, cs.multi_advanced)
     want = cs._advanced(g, None, src, gr, False, False, "keepall", False, False, O.multi_advanced)
+    for ours, ref in ((r.voltage, want.voltage), (r.current, want.current)):
+        np.testing.assert_allclose(ours, ref, rtol=1e-9, atol=1e-11 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("all_to_one", [False, True])
+def test_plain_grid_problems_on_the_raster_route(all_to_one):
+    # no polygons: the problems qualify for the raster solver; "raster" forces it, the oracle checks it
+    rng = np.random.default_rng(70 + all_to_one)
+    ny, nx = 30, 34
+    g = np.exp(rng.normal(size=(ny, nx)))
+    g[rng.random((ny, nx)) < 0.15] = 0
+    pm = np.zeros((ny, nx))
+    pm.flat[rng.choice(ny * nx, size=5, replace=False)] = np.arange(1, 6)
+    flags = dict(habitat_is_resistance=False, voltage_maps=True, current_maps=True, max_map=True)
+    r = cs.circuitscape_one_to_all(g, pm, all_to_one=all_to_one, problem_solver="raster", **flags)
+    maps = {}
+
+    def emit(n, volt, cur):
+        if volt is not None:
+            maps[("voltage", n)] = volt
+        if cur is not None:
+            maps[("current", n)] = cur
+
+    opts = {"volt_maps": True, "cur_maps": True, "cum": True, "max": True, "focal_zero": False}
+    want = cs._one_to_all(g, None, cs._points_from_map(pm), None, None, not all_to_one, False, False, opts, emit,
+                          O.multi_advanced)
+    np.testing.assert_allclose(r.resistances, want.resistances, rtol=1e-9, atol=1e-12)
+    scale = np.abs(want.cum_current).max()
+    np.testing.assert_allclose(r.cum_current, want.cum_current, rtol=1e-9, atol=1e-11 * scale)
+    assert set(r.maps) == set(maps)
+    for k, v in maps.items():
+        np.testing.assert_allclose(r.maps[k], v, rtol=1e-9, atol=1e-11 * max(np.abs(v).max(), 1e-300))
+
+
+def test_plain_grid_advanced_with_finite_grounds_on_the_raster_route():
+    rng = np.random.default_rng(80)
+    ny, nx = 40, 36
+    g = 10 ** rng.uniform(0, 2, size=(ny, nx))
+    g[rng.random((ny, nx)) < 0.1] = 0
+    src = np.zeros((ny, nx))
+    src.flat[rng.choice(ny * nx, 4, replace=False)] = [1.0, 2.0, 0.5, 1.5]
+    gr = np.zeros((ny, nx))
+    cand = np.flatnonzero(src.ravel() == 0)
+    gr.flat[rng.choice(cand, 3, replace=False)] = [np.inf, 0.7, 3.0]
+    r = cs._advanced(g, None, src, gr, False, False, "keepall", False, False,
+                     lambda *a: cs.multi_advanced(*a, problem_solver="raster"))
+    want = cs._advanced(g, None, src, gr, False, False, "keepall", False, False, O.multi_advanced)
+    assert r.maps["solved"] == want.maps["solved"]
     for ours, ref in ((r.voltage, want.voltage), (r.current, want.current)):
         np.testing.assert_allclose(ours, ref, rtol=1e-9, atol=1e-11 * np.abs(ref).max())
