@@ -379,6 +379,100 @@ def bench_pairwise(args, rank, world, local, d):
     d.close()
 
 
+O2A_METRIC = "Circuitscape one-to-all: problems/s (unit current from one focal point, the others direct grounds)"
+
+
+def bench_one_to_all(args, rank, world, local, d):
+    """Circuitscape's one-to-all mode with current maps on the pairwise_256 raster and its 24 focal points (24
+    problems).  A step is one lsb_rasters call over the 24 problem rasters (the route the package takes on a plain
+    grid), inputs resident on the device; the node-graph route (lsb_graph_solve) is timed beside it."""
+    import torch
+    from landschaft_b200 import circuitscape as cs, raster as RA, synthetic
+    r, pm = synthetic.pairwise_256(rank)
+    dev = torch.device("cuda", local)
+    g = cs.habitat_conductance(np.where(np.isnan(r), cs.NODATA, r))
+    fp = cs._points_from_map(pm)
+    rows, cols = fp.cells
+    cells = rows * g.shape[1] + cols
+    npnt = len(cells)
+    ncell = g.size
+    # problem k: unit source at point k, every other point a direct ground (all points lie in one component)
+    S = torch.zeros(npnt * ncell, dtype=torch.float64, device=dev)
+    GR = torch.zeros_like(S)
+    for k in range(npnt):
+        S[k * ncell + int(cells[k])] = 1.0
+        others = torch.from_numpy(k * ncell + np.delete(cells, k)).to(dev)
+        GR[others] = np.inf
+    G = torch.from_numpy(np.ascontiguousarray(g).ravel()).to(dev).repeat(npnt)
+    rp = RA.raster_params(four_neighbors=False, tol=1e-12)
+    shapes = [g.shape] * npnt
+    _, _, rst = RA.run_rasters(G, S, GR, shapes, rp)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for _ in range(args.warmup):
+        RA.run_rasters(G, S, GR, shapes, rp, want_stats=False)
+    clocks = Clocks(local)
+    d.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    times = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        RA.run_rasters(G, S, GR, shapes, rp, want_stats=False)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+    clk = clocks.stop()
+    d.barrier()
+    T = d.max(sum(times))
+    # end to end through the public call, and the node-graph route over the same problems
+    kw = dict(current_maps=True, device=dev)
+    res = cs.circuitscape_one_to_all(r, pm, **kw)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = cs.circuitscape_one_to_all(r, pm, **kw)
+    TE = d.max(time.perf_counter() - t0)
+    cs.circuitscape_one_to_all(r, pm, problem_solver="graph", **kw)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    resg = cs.circuitscape_one_to_all(r, pm, problem_solver="graph", **kw)
+    TG = d.max(time.perf_counter() - t0)
+    cpu = None
+    err = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, str(Path(__file__).resolve().parent / "oracle"))
+        import circuitscape_oracle as O
+        opts = {"volt_maps": False, "cur_maps": True, "cum": True, "max": False, "focal_zero": False}
+        t0 = time.perf_counter()
+        want = cs._one_to_all(g, None, fp, None, None, True, False, False, opts, lambda *a: None, O.multi_advanced)
+        dt = time.perf_counter() - t0
+        err = float(np.max(np.abs(res.resistances[:, 1] - want.resistances[:, 1]) / np.abs(want.resistances[:, 1])))
+        cpu = {"value": npnt / dt, "unit": "problems/s", "cores": 1, "kind": "port",
+               "sample": f"the oracle: all {npnt} problems, each a sparse LU (scipy SuperLU, one thread) of the "
+                        "component, with node currents and the cum map (the graph built with plain loops)"}
+    if rank == 0:
+        line = {"metric": O2A_METRIC, "value": world * npnt * args.steps / T, "unit": "problems/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * T / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 CG + f64 refinement", "data": "synthetic (the pairwise_256 raster and focal points)",
+                "config": {"workload": "one_to_all_256", "cells": int(ncell), "problems": npnt, "neighbours": 8,
+                           "l2": "flushed between timed steps (256 MiB write)", "tol": 1e-12},
+                "solver": "lsb_rasters (FP32 CG, multigrid, FP64 refinement)",
+                "cg_iterations": {"mean": rst.iters_total / max(rst.n_solved, 1), "max": rst.iters_max},
+                "e2e": {"value": world * npnt / TE, "unit": "problems/s",
+                        "h2d_bytes_per_step": int(2 * 8 * ncell), "d2h_bytes_per_step": int(npnt * 2 * 8 * ncell),
+                        "includes": "host graph build, problem construction, all per-point current maps"},
+                "graph_route_e2e": {"value": world * npnt / TG, "unit": "problems/s",
+                                    "solver": "lsb_graph_solve (FP64 Jacobi CG)",
+                                    "max_rel_diff_vs_raster_route": float(np.max(
+                                        np.abs(resg.resistances[:, 1] - res.resistances[:, 1])
+                                        / np.abs(res.resistances[:, 1])))},
+                "max_rel_err_vs_oracle": err, "clocks": clk, "gpu_launches": args.steps, "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    d.close()
+
+
 def bench_advanced(args, rank, world, local, d):
     """The advanced-mode batch: 4096 rasters of sides U{64..512}, log-uniform resistance in [1, 1000], one unit
     source and one direct ground each, 4 neighbours; a step is one launch over the whole batch."""
@@ -519,6 +613,8 @@ def main():
         return bench_advanced(args, rank, world, local, d)
     if args.workload == "pairwise_256":
         return bench_pairwise(args, rank, world, local, d)
+    if args.workload == "one_to_all_256":
+        return bench_one_to_all(args, rank, world, local, d)
     r, s, kw = synthetic.WORKLOADS[args.workload](rank)
     if args.crop:
         y0, x0 = (r.shape[0] - args.crop) // 2, (r.shape[1] - args.crop) // 2
