@@ -322,7 +322,11 @@ def _average(x, y, diagonal: bool, resistances: bool):
 
 
 def raster_graph(gmap: np.ndarray, polymap: np.ndarray | None, avg_resistances: bool,
-                 four_neighbors: bool) -> RasterGraph:
+                 four_neighbors: bool, *, lite: bool = False) -> RasterGraph:
+    """The node graph.  With ``lite``, a plain grid graph (no node merging cells, average-conductance weights) comes
+    without its CSR arrays (ptr, adj, w and degree are None): its components are the 8- or 4-connected regions of
+    habitat cells, numbered by their smallest node; the raster solvers need nothing more.  Other graphs are built in
+    full either way."""
     ny, nx = gmap.shape
     n = nx * ny
     g = np.ascontiguousarray(gmap, dtype=np.float64).ravel()
@@ -346,6 +350,17 @@ def raster_graph(gmap: np.ndarray, polymap: np.ndarray | None, avg_resistances: 
     nodemap = np.full(n, -1, dtype=np.int64)
     nodemap[on] = inv
     n_nodes = len(uniq)
+    if lite and not avg_resistances and np.count_nonzero(on) == n_nodes and not np.any(on & ~(g > 0)):
+        from scipy import ndimage
+        structure = np.ones((3, 3), dtype=bool) if not four_neighbors else ndimage.generate_binary_structure(2, 1)
+        lab, k = ndimage.label(nodemap.reshape(ny, nx) >= 0, structure=structure)
+        node_lab = np.empty(n_nodes, dtype=np.int64)
+        node_lab[nodemap[on]] = lab.ravel()[on] - 1
+        _, first = np.unique(node_lab, return_index=True)
+        rank = np.empty(k, dtype=np.int64)
+        rank[np.argsort(first)] = np.arange(k)
+        return RasterGraph(nx, ny, n_nodes, nodemap, None, None, None, None, rank[node_lab] if k else node_lab, int(k),
+                           bool(four_neighbors), bool(avg_resistances), False)
 
     # edges in column-major cell order: right, below, below right, above right; both orientations
     ys, xs = np.divmod(cm, nx)
@@ -638,6 +653,10 @@ def raster_pairwise(graph: RasterGraph, gmap: np.ndarray, points: np.ndarray, ex
         raise ValueError("the raster pair solver needs a plain grid graph (no short-circuit regions, average "
                          f"conductances, sides up to {MAX_RASTER_SIDE})")
     on_rasters = pair_solver == "raster" or (pair_solver == "auto" and raster_route(graph))
+    if not on_rasters and graph.ptr is None:
+        # a lite graph (no node merging cells): its node map does not depend on the polygons, so the full graph
+        # without them is the same graph
+        graph = raster_graph(gmap, None, graph.avg_resistances, graph.four_neighbors)
     dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
     params = graph_params(tol)
     stats = stats if stats is not None else GraphSolveStats()
@@ -880,7 +899,7 @@ def _run_regions(g, poly, points: FocalPoints, excluded_ids: set, four, avg, o: 
             if ex[i, j] or ex[j, i]:
                 continue
             pm = region_polymap(poly, ncell, cells, ids, int(pts[i]), int(pts[j])).reshape(shape)
-            graph = raster_graph(g, pm, avg, four)
+            graph = raster_graph(g, pm, avg, four, lite=pair_solver != "graph")
             nodes = np.array([graph.nodemap[cells[np.flatnonzero(ids == pts[e])[0]]] for e in (i, j)])
             got = []
             r2, c2, m2 = raster_pairwise(graph, g, nodes, np.zeros((2, 2), dtype=bool), o,
@@ -908,7 +927,7 @@ def _run_pairwise(g, poly, points: FocalPoints, excluded_ids: set, four, avg, o:
                   pair_solver="auto"):
     if points.has_regions:
         return _run_regions(g, poly, points, excluded_ids, four, avg, o, emit, tol, device, pair_solver)
-    graph = raster_graph(g, poly, avg, four)
+    graph = raster_graph(g, poly, avg, four, lite=pair_solver != "graph")
     rows, cols = points.cells
     cells = rows * g.shape[1] + cols
     ok = (cells >= 0) & (cells < g.size)
@@ -1189,7 +1208,7 @@ def multi_advanced(g, poly, avg: bool, four: bool, problems, policy: str, *, tol
     where it applies)."""
     if problem_solver not in ("auto", "graph", "raster"):
         raise ValueError('problem_solver must be "auto", "graph" or "raster"')
-    graph = raster_graph(g, poly, avg, four)
+    graph = raster_graph(g, poly, avg, four, lite=problem_solver != "graph")
     srcs, gnds, only = [], [], []
     for q in problems:
         srcs.append(node_sums(graph, q["src_cells"], q["src_vals"]))
@@ -1209,6 +1228,8 @@ def multi_advanced(g, poly, avg: bool, four: bool, problems, policy: str, *, tol
     if problem_solver == "raster":
         raise ValueError("the raster problem solver needs a plain grid graph and problems without a node that has "
                          "both a source and a ground")
+    if graph.ptr is None:  # a lite graph: the full one (without the polygons, which do not change it)
+        graph = raster_graph(g, None, avg, four)
     return graph.nodemap.reshape(g.shape), advanced_many(graph, srcs, gnds, only, policy, tol=tol, device=device,
                                                          stats=stats)
 

@@ -300,3 +300,21 @@ def test_problem_solver_option():
     poly[2:4, 1:3] = 1
     with pytest.raises(ValueError, match="plain grid"):  # merged nodes: not for the raster solver
         cs.multi_advanced(g, poly, False, False, [prob], "keepall", problem_solver="raster")
+
+
+@pytest.mark.parametrize("four", [False, True])
+def test_lite_graph_equals_the_full_graph(four):
+    rng = np.random.default_rng(12 + four)
+    for trial in range(60):
+        ny, nx = (int(v) for v in rng.integers(1, 25, 2))
+        g = np.exp(rng.normal(size=(ny, nx)))
+        g[rng.random((ny, nx)) < rng.uniform(0, 0.6)] = 0
+        a = cs.raster_graph(g, None, False, four)
+        b = cs.raster_graph(g, None, False, four, lite=True)
+        assert b.ptr is None and (a.n_nodes, a.n_comp) == (b.n_nodes, b.n_comp)
+        np.testing.assert_array_equal(a.nodemap, b.nodemap)
+        np.testing.assert_array_equal(a.comp, b.comp)
+    poly = np.zeros((5, 5), dtype=np.int64)
+    poly[1:3, 1:3] = 1
+    assert cs.raster_graph(np.ones((5, 5)), poly, False, four, lite=True).ptr is not None  # merged: built in full
+    assert cs.raster_graph(np.ones((5, 5)), None, True, four, lite=True).ptr is not None  # series weights: in full
