@@ -318,3 +318,25 @@ def test_lite_graph_equals_the_full_graph(four):
     poly[1:3, 1:3] = 1
     assert cs.raster_graph(np.ones((5, 5)), poly, False, four, lite=True).ptr is not None  # merged: built in full
     assert cs.raster_graph(np.ones((5, 5)), None, True, four, lite=True).ptr is not None  # series weights: in full
+
+
+def test_wide_rasters_fall_back_to_the_full_graph(monkeypatch):
+    # over 1024 cells wide: "auto" cannot use the raster solver, so the lite graph is rebuilt in full for the
+    # node-graph kernel; the results equal those of pair_solver="graph" (the solve is a deterministic fake)
+    seen = []
+
+    def fake(graph, members, ground, src, dst, want_currents, params, stats, dev):
+        seen.append(graph.ptr is not None)
+        r = np.random.default_rng(int(src.sum() * 3 + dst.sum()))
+        return r.normal(size=(len(src), len(members))), np.abs(r.normal(size=(len(src), len(members))))
+
+    monkeypatch.setattr(cs, "_solve_component", fake)
+    rng = np.random.default_rng(4)
+    g = np.exp(rng.normal(size=(3, 1100)))
+    pm = np.zeros(g.shape)
+    pm[0, 5], pm[2, 600], pm[1, 1090] = 1, 2, 3
+    a = cs.circuitscape_pairwise(g, pm, habitat_is_resistance=False, cum_map=True, device="cpu")
+    b = cs.circuitscape_pairwise(g, pm, habitat_is_resistance=False, cum_map=True, device="cpu", pair_solver="graph")
+    assert seen and all(seen)
+    np.testing.assert_array_equal(a.resistances, b.resistances)
+    np.testing.assert_array_equal(a.cum_current, b.cum_current)
