@@ -32,10 +32,11 @@ struct GArgs {
     JobStat *jstat;
 };
 
-// y = A v on the unknowns (the ground's row is 0; v at the ground is 0).  Entries whose column is out of range are
-// skipped and counted in `bad`.
+// y = A v on the unknowns (the ground's row is 0; v at the ground is 0); returns this thread's part of v.y, summed in
+// row order.  Entries whose column is out of range are skipped and counted in `bad`.
 template <int NT>
-__device__ __forceinline__ void spmv(const GArgs &a, const double *v, double *y, int &bad) {
+__device__ __forceinline__ double spmv(const GArgs &a, const double *v, double *y, int &bad) {
+    double dot = 0.0;
     for (int i = threadIdx.x; i < a.n; i += NT) {
         double s = 0.0;
         if (i != a.ground) {
@@ -50,7 +51,9 @@ __device__ __forceinline__ void spmv(const GArgs &a, const double *v, double *y,
             }
         }
         y[i] = s;
+        dot += v[i] * s;
     }
+    return dot;
 }
 
 // Right-hand side: +1 at dst, -1 at src, 0 at the ground.
@@ -90,10 +93,8 @@ __device__ void solve_job(const GArgs &a, int64_t j, double *r, double *p, doubl
     int it = 0, stall = 0;
     for (int cycle = 0; cycle < kMaxRestarts; ++cycle) {
         while (it < a.max_iter && rr > goal) {
-            spmv<NT>(a, p, q, bad);
+            const double ppq = spmv<NT>(a, p, q, bad);  // this thread's part of p.q, in row order
             __syncthreads();
-            double ppq = 0.0;
-            for (int i = threadIdx.x; i < n; i += NT) ppq += p[i] * q[i];
             const double pq = block_sum2<NT>(ppq, 0.0, red).x;
             if (!(pq > 0.0)) break;  // breakdown: the true residual decides below
             const double alpha = rz / pq;

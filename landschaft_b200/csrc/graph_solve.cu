@@ -38,11 +38,12 @@ struct SArgs {
     JobStat *jstat;
 };
 
-// y = A v on the unknowns (rows of direct grounds are 0; v is 0 there).  Entries whose column is out of range are
-// skipped and counted in `bad`.
+// y = A v on the unknowns (rows of direct grounds are 0; v is 0 there); returns this thread's part of v.y, summed in
+// row order.  Entries whose column is out of range are skipped and counted in `bad`.
 template <int NT>
-__device__ __forceinline__ void spmv(const SArgs &a, const double *dg, const uint8_t *mask, const double *v,
-                                     double *y, int &bad) {
+__device__ __forceinline__ double spmv(const SArgs &a, const double *dg, const uint8_t *mask, const double *v,
+                                       double *y, int &bad) {
+    double dot = 0.0;
     for (int i = threadIdx.x; i < a.n; i += NT) {
         double s = 0.0;
         if (!mask[i]) {
@@ -57,7 +58,9 @@ __device__ __forceinline__ void spmv(const SArgs &a, const double *dg, const uin
             }
         }
         y[i] = s;
+        dot += v[i] * s;
     }
+    return dot;
 }
 
 template <int NT>
@@ -118,10 +121,8 @@ __device__ void solve_problem(const SArgs &a, int64_t j, double *scr, double2 *r
     int it = 0, stall = 0;
     for (int cycle = 0; cycle < kMaxRestarts; ++cycle) {
         while (it < a.max_iter && rr > goal) {
-            spmv<NT>(a, dg, mask, p, q, bad);
+            const double ppq = spmv<NT>(a, dg, mask, p, q, bad);  // this thread's part of p.q, in row order
             __syncthreads();
-            double ppq = 0.0;
-            for (int i = threadIdx.x; i < n; i += NT) ppq += p[i] * q[i];
             const double pq = block_sum2<NT>(ppq, 0.0, red).x;
             if (!(pq > 0.0)) break;  // breakdown: the true residual decides below
             const double alpha = rz / pq;
