@@ -1539,6 +1539,7 @@ DEFAULTS = {
     "source_file": "(Browse for a current source file)", "ground_file": "(Browse for a ground point file)",
     "ground_file_is_resistances": "True", "use_unit_currents": "False", "use_direct_grounds": "False",
     "remove_src_or_gnd": "keepall", "use_variable_source_strengths": "False", "variable_source_file": "None",
+    "output_file": "(Choose a base name for output files)", "write_as_tif": "False",
 }
 SCENARIOS = {"pairwise": "pairwise", "Pairwise": "pairwise", "advanced": "advanced", "Advanced": "advanced",
              "one-to-all": "one-to-all", "one_to_all": "one-to-all", "all-to-one": "all-to-one",
@@ -1579,16 +1580,70 @@ def _resolve(name: str, base: Path) -> Path:
     return q if q.exists() else p
 
 
-def circuitscape_ini(path, *, write_outputs: bool = False, tol: float = 1e-13, device=None,
+def _write_grid(prefix: str, values: np.ndarray, meta: RasterMeta) -> None:
+    """An ESRI ASCII grid (Circuitscape's header, NoData -9999, NaN written as NoData); values as Python writes
+    floats (repr), so that reading the file back gives the same doubles."""
+    out = np.where(np.isnan(values), NODATA, values)
+    with open(prefix + ".asc", "w", encoding="utf-8") as f:
+        f.write(f"ncols         {meta.ncols}\nnrows         {meta.nrows}\n")
+        f.write(f"xllcorner     {meta.xllcorner!r}\nyllcorner     {meta.yllcorner!r}\n")
+        f.write(f"cellsize      {meta.cellsize!r}\nNODATA_value  -9999\n")
+        for row in out:
+            f.write(" ".join(repr(float(v)) for v in row) + "\n")
+
+
+def _write_matrix(path: str, a: np.ndarray) -> None:
+    with open(path, "w", encoding="utf-8") as f:
+        for row in np.atleast_2d(a):
+            f.write(" ".join(repr(float(v)) for v in row) + "\n")
+
+
+def _output_prefix(cfg) -> str:
+    out = cfg["output_file"]
+    if _unset(out):
+        raise ValueError("output_file is not set")
+    if _flag(cfg, "write_as_tif"):
+        raise NotImplementedError("write_as_tif: only ESRI ASCII grids are written")
+    Path(out).parent.mkdir(parents=True, exist_ok=True)
+    return out.split(".out")[0]
+
+
+def _write_outputs(cfg, scenario: str, result: CircuitscapeResult, meta: RasterMeta) -> None:
+    """Circuitscape's output files (circuitscape.py:1261-1286): the configuration in output_file, the maps next
+    to it (the per-pair and per-point maps are written as they are computed), the resistance matrices."""
+    prefix = _output_prefix(cfg)
+    with open(cfg["output_file"], "w", encoding="utf-8") as f:
+        for k, v in cfg.items():
+            f.write(f"{k} = {v}\n")
+    if scenario == "advanced":
+        if _flag(cfg, "write_volt_maps"):
+            _write_grid(prefix + "_voltmap", result.voltage, meta)
+        if _flag(cfg, "write_cur_maps") or _flag(cfg, "write_cum_cur_map_only"):
+            _write_grid(prefix + "_curmap", result.current, meta)
+        return
+    if result.cum_current is not None:
+        _write_grid(prefix + "_cum_curmap", result.cum_current, meta)
+    if result.max_current is not None:
+        _write_grid(prefix + "_max_curmap", result.max_current, meta)
+    if scenario == "pairwise":
+        r = result.resistances
+        _write_matrix(prefix + "_resistances.out", r)
+        fp = r[1:, 0]
+        three = [(fp[i], fp[j], r[j + 1, i + 1]) for i in range(len(fp)) for j in range(i + 1, len(fp))]
+        _write_matrix(prefix + "_resistances_3columns.out", np.array(three).reshape(-1, 3))
+
+
+def circuitscape_ini(path, *, write_outputs: bool = True, tol: float = 1e-13, device=None,
                      pair_solver: str = "auto", problem_solver: str = "auto", _solver=None) -> CircuitscapeResult:
     """Run a Circuitscape INI file on rasters (scenarios pairwise, advanced, one-to-all and all-to-one), as the
     reference's ``circuitscape_ini`` does (circuitscape.py:1039-1213); paths are read from the working directory, or
     else next to the INI file.  ``maps`` are keyed as Circuitscape names its files (``voltmap_<id1>_<id2>``,
-    ``curmap_<id>``...).  Writing output files is not supported (``write_outputs`` must be False).  ``_solver``
+    ``curmap_<id>``...).  With ``write_outputs`` the maps go next to ``output_file`` as Circuitscape names them
+    (``<base>_voltmap``, ``<base>_curmap``..., ESRI ASCII grids; the per-pair and per-point maps are then written
+    instead of kept in ``maps``), the resistances to ``<base>_resistances.out`` and the configuration to
+    ``output_file``.  ``_solver``
     replaces the GPU solve of the advanced-mode scenarios (a callable with the signature of multi_advanced without
     its keywords)."""
-    if write_outputs:
-        raise NotImplementedError("writing Circuitscape output files is not supported")
     path = Path(path)
     base = path.resolve().parent
     cfg = {**DEFAULTS, **parse_config(path)}
@@ -1630,11 +1685,15 @@ def circuitscape_ini(path, *, write_outputs: bool = False, tol: float = 1e-13, d
     solver = _solver if _solver is not None else (
         lambda *a: multi_advanced(*a, tol=tol, device=device, problem_solver=problem_solver))
 
+    prefix = _output_prefix(cfg) if write_outputs else None
     if scenario == "advanced":
         src, gnd = _source_and_ground(need("source_file"), need("ground_file"), meta,
                                       _flag(cfg, "ground_file_is_resistances"))
-        return _advanced(g, poly, src, gnd, four, avg, policy, _flag(cfg, "use_unit_currents"),
-                         _flag(cfg, "use_direct_grounds"), solver)
+        result = _advanced(g, poly, src, gnd, four, avg, policy, _flag(cfg, "use_unit_currents"),
+                           _flag(cfg, "use_direct_grounds"), solver)
+        if write_outputs:
+            _write_outputs(cfg, scenario, result, meta)
+        return result
 
     points = read_point_map(need("point_file"), meta)
     pairs = read_included_pairs(need("included_pairs_file")) if _flag(cfg, "use_included_pairs") else None
@@ -1650,14 +1709,19 @@ def circuitscape_ini(path, *, write_outputs: bool = False, tol: float = 1e-13, d
                 "focal_zero": _flag(cfg, "set_focal_node_currents_to_zero")}
 
         def emit_point(n, volt, curmap):
-            if volt is not None:
-                maps[f"voltmap_{n}"] = volt
-            if curmap is not None:
-                maps[f"curmap_{n}"] = curmap
+            for kind, grid in (("voltmap", volt), ("curmap", curmap)):
+                if grid is None:
+                    continue
+                if write_outputs:
+                    _write_grid(f"{prefix}_{kind}_{n}", grid, meta)
+                else:
+                    maps[f"{kind}_{n}"] = grid
 
         result = _one_to_all(g, poly, points, strengths, pairs, scenario == "one-to-all", four, avg, opts,
                              emit_point, solver)
         result.maps = maps
+        if write_outputs:
+            _write_outputs(cfg, scenario, result, meta)
         return result
 
     points, excluded = _apply_included_pairs(points, pairs)
@@ -1671,10 +1735,16 @@ def circuitscape_ini(path, *, write_outputs: bool = False, tol: float = 1e-13, d
 
     def emit(ci, cj, volt, curmap):
         name = f"_{int(ids[ci])}_{int(ids[cj])}"
-        if volt is not None:
-            maps["voltmap" + name] = volt
-        if curmap is not None:
-            maps["curmap" + name] = curmap
+        for kind, grid in (("voltmap", volt), ("curmap", curmap)):
+            if grid is None:
+                continue
+            if write_outputs:
+                _write_grid(f"{prefix}_{kind}{name}", grid, meta)
+            else:
+                maps[kind + name] = grid
 
     res, cum, mx, stats = _run_pairwise(g, poly, points, excluded, four, avg, o, emit, tol, device, pair_solver)
-    return CircuitscapeResult(resistances=res, cum_current=cum, max_current=mx, maps=maps, stats=stats)
+    result = CircuitscapeResult(resistances=res, cum_current=cum, max_current=mx, maps=maps, stats=stats)
+    if write_outputs:
+        _write_outputs(cfg, scenario, result, meta)
+    return result

@@ -213,12 +213,12 @@ def check_one_to_all(name, r, rtol=1e-11):
 
 @pytest.mark.parametrize("ini", ADVANCED_CASES)
 def test_oracle_matches_circuitscape_advanced(ini, in_cs):
-    check_advanced(Path(ini).stem, cs.circuitscape_ini(ini, _solver=O.multi_advanced))
+    check_advanced(Path(ini).stem, cs.circuitscape_ini(ini, write_outputs=False, _solver=O.multi_advanced))
 
 
 @pytest.mark.parametrize("ini", ONE_TO_ALL_CASES + ALL_TO_ONE_CASES)
 def test_oracle_matches_circuitscape_one_to_all(ini, in_cs):
-    check_one_to_all(Path(ini).stem, cs.circuitscape_ini(ini, _solver=O.multi_advanced))
+    check_one_to_all(Path(ini).stem, cs.circuitscape_ini(ini, write_outputs=False, _solver=O.multi_advanced))
 
 
 def test_mode_case_counts():
@@ -340,3 +340,21 @@ def test_wide_rasters_fall_back_to_the_full_graph(monkeypatch):
     assert seen and all(seen)
     np.testing.assert_array_equal(a.resistances, b.resistances)
     np.testing.assert_array_equal(a.cum_current, b.cum_current)
+
+
+def test_one_to_all_ini_writes_outputs(tmp_path, in_cs):
+    # as Circuitscape writes them: the configuration, the cum map and every point's maps, read back bitwise
+    src = CS / "input/raster/one_to_all/1/oneToAllVerify1.ini"
+    text = src.read_text()
+    out = cs.parse_config(src)["output_file"]
+    ini = tmp_path / "run.ini"
+    ini.write_text(text.replace(out, (tmp_path / "o2a.out").as_posix()))
+    r = cs.circuitscape_ini(ini, _solver=O.multi_advanced)
+    assert r.maps == {} and (tmp_path / "o2a.out").exists()
+    cum, _ = cs.read_raster(tmp_path / "o2a_cum_curmap.asc")
+    np.testing.assert_array_equal(cum, r.cum_current)
+    want = {p.stem for p in tmp_path.glob("o2a_*map_*.asc")}
+    z = np.load(CS / "modes.npz")
+    theirs = {"o2a_" + k.split("/")[1][:-4] for k in z.files if k.startswith("oneToAllVerify1/")
+              and k.split("/")[1].startswith(("curmap_", "voltmap_"))}
+    assert want == theirs

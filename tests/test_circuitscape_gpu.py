@@ -31,7 +31,7 @@ def in_cs(monkeypatch):
 @pytest.mark.parametrize("pair_solver", ["auto", "graph"])
 @pytest.mark.parametrize("name", POINT_CASES + REGION_CASES)
 def test_pairwise_matches_circuitscape(name, pair_solver, in_cs):
-    r = cs.circuitscape_ini(ini_path(name), pair_solver=pair_solver)
+    r = cs.circuitscape_ini(ini_path(name), write_outputs=False, pair_solver=pair_solver)
     check_against_golden(name, r.resistances, r.cum_current, r.max_current, r.maps)
     assert r.stats.failures == 0 and r.stats.jobs > 0
 
@@ -223,14 +223,14 @@ def test_iteration_cap_reports_failure():
 @pytest.mark.parametrize("ini", ADVANCED_CASES)
 def test_advanced_matches_circuitscape(ini, problem_solver, in_cs):
     # the reference's bar, rtol 1e-9
-    check_advanced(Path(ini).stem, cs.circuitscape_ini(ini, problem_solver=problem_solver))
+    check_advanced(Path(ini).stem, cs.circuitscape_ini(ini, write_outputs=False, problem_solver=problem_solver))
 
 
 @pytest.mark.parametrize("problem_solver", ["auto", "graph"])
 @pytest.mark.parametrize("ini", ONE_TO_ALL_CASES + ALL_TO_ONE_CASES)
 def test_one_to_all_matches_circuitscape(ini, problem_solver, in_cs):
     # the reference's bar is 1e-11 for its direct solver; the GPU's iterative solve is held to 1e-9
-    check_one_to_all(Path(ini).stem, cs.circuitscape_ini(ini, problem_solver=problem_solver), rtol=1e-9)
+    check_one_to_all(Path(ini).stem, cs.circuitscape_ini(ini, write_outputs=False, problem_solver=problem_solver), rtol=1e-9)
 
 
 @pytest.mark.parametrize("policy", cs.POLICIES)
@@ -381,3 +381,17 @@ def test_plain_grid_advanced_with_finite_grounds_on_the_raster_route():
     assert r.maps["solved"] == want.maps["solved"]
     for ours, ref in ((r.voltage, want.voltage), (r.current, want.current)):
         np.testing.assert_allclose(ours, ref, rtol=1e-9, atol=1e-11 * np.abs(ref).max())
+
+
+def test_pairwise_ini_writes_outputs(tmp_path, in_cs):
+    src = CS / "input/raster/pairwise/1/sgVerify1.ini"
+    out = cs.parse_config(src)["output_file"]
+    ini = tmp_path / "run.ini"
+    ini.write_text(src.read_text().replace(out, (tmp_path / "pw.out").as_posix()))
+    r = cs.circuitscape_ini(ini)
+    np.testing.assert_array_equal(np.loadtxt(tmp_path / "pw_resistances.out"), r.resistances)
+    three = np.loadtxt(tmp_path / "pw_resistances_3columns.out")
+    n = len(r.resistances) - 1
+    assert three.shape == (n * (n - 1) // 2, 3)
+    np.testing.assert_array_equal(cs.read_raster(tmp_path / "pw_cum_curmap.asc")[0], r.cum_current)
+    assert (tmp_path / "pw_curmap_1_2.asc").exists() and r.maps == {}
